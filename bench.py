@@ -1,0 +1,394 @@
+"""Benchmark: batched mixed-precision refactor + solve on one B200 (or N).
+
+Workload (one step): the 63x64 power-grid MNA matrix plus 18 Vdd pad rows
+(n = 4050), 50 Newton refactorizations on the same pattern with element
+values perturbed log-normally (sigma = 0.1), each followed by a full solve:
+fp32 factors (frozen pivots) + fp64 GMRES-IR (restart 30, rtol 1e-10), all
+50 systems in one persistent launch.  `value` counts only systems whose
+solution is within rel-L2 1e-6 of the fp64 oracle (checked after timing).
+
+Also reported: the plain fp64 GPU path on the same inputs (per request and
+batched), p50/p99 single-request latency, the end-to-end figure through the
+public API with host buffers (e2e), the roofline of the batch kernel, and
+the reference's CPU path (cpu_baseline).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 launch with torch.distributed.run (one rank per GPU); ranks run
+independent replicas of the workload (no exchange), value = all ranks'
+systems / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "refactor+solves/s at rel err ≤1e-6 (mixed vs fp64 GPU); p50/p99 solve latency"
+UNIT = "refactor+solves/s"
+NSYS = 50
+WORKLOAD = ("power-grid MNA n=4050 (63x64 mesh + 18 Vdd pads), 50 Newton refactors on one "
+            "pattern (log-normal sigma=0.1 element perturbation), fp32 factor + fp64 GMRES-IR "
+            "(restart 30, rtol 1e-10), one persistent launch per step")
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def algorithmic_bytes(info, stats, vs=4):
+    """Compulsory bytes of one refactor + GMRES-IR solve (per system), from
+    the pattern sizes and the iteration counts the kernel reported:
+      refactor  nnz(A)(8+4) + (n+1)4 + nnz(L+U)(vs+4) + 4n
+      trisolve  nnz(L+U)(vs+4) + 2(n+1)4 + 3*8n
+      SpMV      nnz(A)(s_v+4) + (n+1)4 + 8n + 8n
+      inner j   SpMV(vs) + trisolve + 2 passes (j+1) 2*8n
+      outer     SpMV(fp64) + 3*8n, plus one trisolve per correction."""
+    n, nnz = info["n"], info["nnz_a"]
+    lu = info["cap"]
+    refactor = nnz * 12 + (n + 1) * 4 + lu * (vs + 4) + 4 * n
+    tri = lu * (vs + 4) + 2 * (n + 1) * 4 + 3 * 8 * n
+    spmv_in = nnz * (vs + 4) + (n + 1) * 4 + 16 * n
+    spmv64 = nnz * 12 + (n + 1) * 4 + 16 * n
+    total = 0
+    for st in stats:
+        b = refactor
+        outer = max(st["outer_iters"], 0)
+        inner = max(st["inner_iters"], 0)
+        b += max(st["nres"], 1) * (spmv64 + 3 * 8 * n)
+        if outer:
+            per = inner / outer
+            js = []
+            left = inner
+            for _ in range(outer):
+                c = int(round(per)) if left > per else left
+                js.extend(range(c))
+                left -= c
+            for j in js:
+                b += spmv_in + tri + 2 * (j + 1) * 2 * 8 * n
+            b += outer * tri
+        total += b
+    return total
+
+
+def ref_cpu_worker(args):
+    """One reference CPU factor+solve (compiled reference sources)."""
+    n, Ap, Ai, vals, q, b = args
+    from oracle import oracle
+    t = time.perf_counter()
+    x = oracle.ref_cpu_solve(n, Ap, Ai, vals, q, b)
+    return time.perf_counter() - t, x
+
+
+def cpu_reference_rate(m, vals, q, threads, budget_s=12.0):
+    """Reference CPU path (splu lu_factor + lu_solve_perm, cpu_ref_lu.c) on a
+    bounded sample of the same value sets; returns (systems/s, sample desc, kind)."""
+    from oracle import oracle
+    kind = "reference" if oracle.ref_available() else "port"
+    work = [(m.n, m.Ap, m.Ai, vals[i % len(vals)], q, m.b) for i in range(len(vals))]
+    if threads <= 1:
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            ref_cpu_worker(work[done % len(work)])
+            done += 1
+        el = time.perf_counter() - t0
+        return done / el, f"{done} refactor+solves of the step's value sets, 1 thread, {el:.1f} s", kind
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(threads) as pool:
+        pool.map(ref_cpu_worker, work[:threads])  # warm the workers
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            pool.map(ref_cpu_worker, work)
+            done += len(work)
+        el = time.perf_counter() - t0
+    return done / el, f"{done} refactor+solves of the step's value sets, {threads} processes, {el:.1f} s", kind
+
+
+def setup_dist(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def max_over_ranks(v, world):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args):
+    rank, world, local = setup_dist(args.gpus)
+    if rank != 0:
+        return
+    from luspice_b200 import api, mna
+    from oracle import oracle
+    m = mna.power_grid()
+    vals = m.perturbed(NSYS, seed=4242)
+    q = api.colamd(m.n, m.Ap, m.Ai)
+    threads = os.cpu_count() or 1
+    rate, sample, kind = cpu_reference_rate(m, vals, q, threads, budget_s=max(3.0, 2.0 * args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * NSYS / rate,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "systems_per_step": NSYS,
+                                            "path": "reference CPU lu_factor + lu_solve_perm (cpu_ref_lu.c), COLAMD order from this project"},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = setup_dist(args.gpus)
+    import torch
+    torch.cuda.set_device(local)
+    from luspice_b200 import api, mna
+
+    m = mna.power_grid()
+    vals = m.perturbed(NSYS, seed=4242)
+    P = api.Pattern.from_matrix(m)
+    info = P.info
+    _, q = P.perm()
+    stream = torch.cuda.Stream()
+    rhs = np.tile(m.b, NSYS)
+    B = api.Batch([P] * NSYS, prec=api.MIXED, krylov=30)
+    B.upload(list(vals), rhs, stream=stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step(batch, what=api.RUN_BOTH):
+        batch.run(what, stream=stream, graph=True)
+
+    # Warm-up (captures the graph), then timed steps with an L2 flush between.
+    for _ in range(max(args.warmup, 3)):
+        step(B)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))
+                ev[i][0].record(stream)
+            step(B)
+            with torch.cuda.stream(stream):
+                ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    barrier(world)
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    step_ms = max_over_ranks(statistics.mean(kern_ms), world)
+
+    # Accuracy gate against the fp64 oracle (same value sets).
+    from oracle import oracle
+    xs = B.split(B.download(stream=stream))
+    torch.cuda.synchronize()
+    stats = B.stats(stream=stream)
+    accepted, errs = 0, []
+    for s in range(NSYS):
+        ref = oracle.ref_cpu_solve(m.n, m.Ap, m.Ai, vals[s], q, m.b)
+        e = float(np.linalg.norm(xs[s] - ref) / np.linalg.norm(ref))
+        errs.append(e)
+        accepted += int(e <= 1e-6)
+    value = accepted * world / (step_ms / 1000.0)
+
+    # Roofline of the batch kernel (the only kernel of the step).
+    hbm, peak_kind = peaks()
+    alg = algorithmic_bytes(info, stats, vs=4)
+    achieved = alg / (statistics.mean(kern_ms) / 1000.0) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "batch_kernel_power_grid4050x50.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+
+    # Plain fp64 GPU path on the same inputs: batched, and per request.
+    B64 = api.Batch([P] * NSYS, prec=api.FP64)
+    B64.upload(list(vals), rhs, stream=stream)
+    for _ in range(3):
+        step(B64)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    reps = max(3, args.steps // 2)
+    for _ in range(reps):
+        step(B64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fp64_batched_ms = e0.elapsed_time(e1) / reps
+    x64 = B64.split(B64.download(stream=stream))
+    torch.cuda.synchronize()
+    acc64 = sum(int(np.linalg.norm(x64[s] - oracle.ref_cpu_solve(m.n, m.Ap, m.Ai, vals[s], q, m.b)) /
+                    np.linalg.norm(x64[s]) <= 1e-6) for s in range(NSYS))
+    single = {}
+    lat = {}
+    for prec in (api.FP64, api.MIXED):
+        b1 = api.Batch([P], prec=prec)
+        times = []
+        for s in range(NSYS):
+            b1.upload([vals[s]], [m.b], stream=stream)
+            a, bq = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            b1.run(api.RUN_BOTH, stream=stream)
+            bq.record(stream)
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(bq))
+        single[prec] = statistics.mean(times)
+        lat[prec] = (float(np.percentile(times, 50)), float(np.percentile(times, 99)))
+        b1.close()
+    fp64_per_request_rate = 1000.0 / single[api.FP64]
+
+    # End to end through the public API with pinned host buffers: values and
+    # right-hand sides host->device, one launch, solutions device->host.
+    hv = torch.from_numpy(np.ascontiguousarray(np.concatenate(list(vals)))).pin_memory()
+    hb = torch.from_numpy(np.ascontiguousarray(rhs)).pin_memory()
+    hx = torch.empty(NSYS * m.n, dtype=torch.float64).pin_memory()
+    vals_np, rhs_np, x_np = hv.numpy(), hb.numpy(), hx.numpy()
+    for _ in range(3):
+        B.upload(vals_np, rhs_np, stream=stream)
+        step(B)
+        B.download(out=x_np, stream=stream)
+    torch.cuda.synchronize()
+    ee = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        ee[i][0].record(stream)
+        B.upload(vals_np, rhs_np, stream=stream)
+        step(B)
+        B.download(out=x_np, stream=stream)
+        ee[i][1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(statistics.mean([a.elapsed_time(b) for a, b in ee]), world)
+    h2d = int(vals_np.nbytes + rhs_np.nbytes)
+    d2h = int(x_np.nbytes)
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu:
+            rate, sample, kind = cpu_reference_rate(m, vals, q, 1, budget_s=10.0)
+            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "systems_per_step": NSYS, "n": m.n, "nnz": m.nnz,
+                       "lu_slots": info["cap"], "col_levels": info["ncol_levels"],
+                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                       "graph": True},
+            "accepted": accepted, "max_rel_err": max(errs),
+            "mean_inner_iters": float(np.mean([s["inner_iters"] for s in stats])),
+            "latency_ms": {"mixed_p50": lat[api.MIXED][0], "mixed_p99": lat[api.MIXED][1],
+                           "fp64_p50": lat[api.FP64][0], "fp64_p99": lat[api.FP64][1]},
+            "fp64_gpu": {"per_request_rate": fp64_per_request_rate, "batched_rate": NSYS * 1000.0 / fp64_batched_ms,
+                         "batched_accepted": acc64,
+                         "mixed_batched_over_fp64_per_request": value / world / fp64_per_request_rate,
+                         "mixed_batched_over_fp64_batched": (NSYS * 1000.0 / step_ms) / (NSYS * 1000.0 / fp64_batched_ms)},
+            "e2e": {"value": accepted * world / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "batch_kernel<float,float>", "alg_bytes_per_launch": alg},
+            "gpu_launches": args.steps * B.launch_count(),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+            "wall_s_timed": wall,
+        }
+        print(json.dumps(line), flush=True)
+    B.close()
+    B64.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

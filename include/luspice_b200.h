@@ -1,0 +1,178 @@
+/*
+ * luspice_b200.h - batched refactor-and-solve C-ABI for one B200.
+ *
+ * This interface is added beside the reference's headers (it replaces none
+ * of them): it exposes the pattern cache, the batched persistent launch and
+ * the serving loop that the reference only sketches (src/lu_static.h:73-75
+ * is a stub; batching exists only as benchmarks, src/mp/batch_spmv.cu).
+ *
+ * Model:
+ *   lusp_pattern : one sparsity pattern after host analysis (COLAMD column
+ *                  order, pivoting fp64 LU that fixes P and the L/U pattern,
+ *                  level schedules) and its device-resident static layout.
+ *   lusp_batch   : N systems (pattern + values + right-hand side) processed
+ *                  by one persistent kernel: one CTA per system, systems
+ *                  taken from a device work queue, columns and rows taken in
+ *                  level order inside the CTA.
+ *   lusp_server  : continuous-batching request loop on top of batches.
+ *
+ * Index conventions: CSC inputs are 0-based (Ap[n+1], Ai[nnz] = row, Ax[nnz]
+ * in the same entry order); rows may be unsorted; duplicate entries are
+ * summed.  All pointers are host pointers unless the name says d_.  Every
+ * function returns an int status (LUSP_OK = 0) and never throws.  A stream
+ * argument is a cudaStream_t passed as void* (NULL = legacy default stream).
+ */
+#ifndef LUSPICE_B200_H
+#define LUSPICE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    LUSP_OK = 0,
+    LUSP_ESINGULAR = 1,   /* no nonzero pivot in some column */
+    LUSP_EALLOC = 2,      /* host or device allocation failed */
+    LUSP_EARG = 3,        /* invalid argument */
+    LUSP_ECUDA = 4,       /* a CUDA call failed (see lusp_last_error) */
+    LUSP_ENODEV = 5,      /* no usable sm_100 device */
+    LUSP_EBUSY = 6        /* request not finished (lusp_serve_poll) */
+};
+
+/* Per-system status bits (lusp_sys_stats.status). */
+enum {
+    LUSP_ST_SINGULAR = 1,
+    LUSP_ST_PIVOT_WEAK = 2,
+    LUSP_ST_STAGNATED = 4,
+    LUSP_ST_NOT_CONVERGED = 8,
+    LUSP_ST_NONFINITE = 16,
+    LUSP_ST_WAIT_TIMEOUT = 32,
+    LUSP_ST_CAPACITY = 64,
+    LUSP_ST_ESCALATED = 128   /* result comes from the fp64 path */
+};
+
+enum { LUSP_MIXED = 0, LUSP_FP64 = 1 };
+/* what: bit 1 refactor, bit 2 solve; LUSP_RUN_DIRECT makes the solve a
+ * plain x = Q U^-1 L^-1 P b with the stored factors (no iteration). */
+enum { LUSP_RUN_REFACTOR = 1, LUSP_RUN_SOLVE = 2, LUSP_RUN_BOTH = 3, LUSP_RUN_DIRECT = 4 };
+
+typedef struct lusp_pattern lusp_pattern;
+typedef struct lusp_batch lusp_batch;
+typedef struct lusp_server lusp_server;
+
+typedef struct {
+    int n, nnz_a;
+    long lnnz, unnz, cap;          /* splu-convention counts; cap = merged slots */
+    int ncol_levels, nfwd_levels, nbwd_levels;
+    int max_col, nslices, sell_total;
+    long flops;                    /* multiply-adds of one refactorization */
+    long gathered;                 /* L entries gathered by one refactorization */
+    unsigned long long hash;
+    size_t device_bytes;
+    int singular_col;              /* -1 unless creation failed as singular */
+} lusp_pattern_info;
+
+typedef struct {
+    double min_abs_pivot, min_pivot_ratio, max_abs_u;
+    double res[16];                /* ||b - A x|| / ||b|| history */
+    int nres, inner_iters, outer_iters, status, singular_col, pad_;
+} lusp_sys_stats;
+
+typedef struct {
+    int prec;                      /* LUSP_MIXED (fp32 factors + GMRES-IR) or LUSP_FP64 (direct) */
+    int krylov;                    /* GMRES restart length (default 30, max 64) */
+    int max_outer;                 /* outer corrections (default 3) */
+    double rtol;                   /* ||b-Ax||/||b|| target (default 1e-10) */
+    double inner_rel;              /* inner stop vs current residual (default 1e-8) */
+    double stag_ratio;             /* required residual reduction per outer (default 0.5) */
+    double pivot_tol;              /* frozen-pivot acceptance (default 1e-3) */
+    int block_threads;             /* CTA size (default 256) */
+    int ctas_per_sm;               /* shared-memory plan target (default 2) */
+} lusp_batch_opts;
+
+/* ---- library ---- */
+const char *lusp_last_error(void);
+const char *lusp_version(void);
+int lusp_device_count(void);
+
+/* ---- patterns ---- */
+/* q: column order (NULL -> COLAMD computed here).  Ax: the values used to
+ * choose pivots (the first Newton step).  On LUSP_ESINGULAR *out is NULL
+ * and lusp_last_error names the column. */
+int lusp_pattern_create(int n, const int *Ap, const int *Ai, const double *Ax,
+                        const int *q, lusp_pattern **out);
+void lusp_pattern_destroy(lusp_pattern *p);
+int lusp_pattern_get_info(const lusp_pattern *p, lusp_pattern_info *info);
+/* pinv[orig_row] = position; q[position] = original column. */
+int lusp_pattern_get_perm(const lusp_pattern *p, int *pinv, int *q);
+/* merged columns in position space: cp[n+1], ri[cap], dg[n]. */
+int lusp_pattern_get_structure(const lusp_pattern *p, int *cp, int *ri, int *dg);
+/* column levels (level.c semantics) */
+int lusp_pattern_get_levels(const lusp_pattern *p, int *col_level);
+
+/* ---- host analysis entry points (no device needed) ---- */
+int lusp_colamd(int n_row, int n_col, const int *Ap, const int *Ai,
+                double knob_dense_row, double knob_dense_col, int *q);
+/* Pivoting fp64 LU in splu layout (test and tooling use). Arrays sized by
+ * the caller: pinv[n], Lp[n+1], Up[n+1]; Li/Lx/Ui/Ux with capacities
+ * lcap/ucap (returns LUSP_EALLOC with *lnnz/*unnz set when too small).
+ * Returns LUSP_OK or LUSP_ESINGULAR (*singular_col set). */
+int lusp_pivot_factor(int n, const int *Ap, const int *Ai, const double *Ax,
+                      const int *q, double tol, int *pinv,
+                      int *Lp, int *Li, double *Lx, long lcap,
+                      int *Up, int *Ui, double *Ux, long ucap,
+                      long *lnnz, long *unnz, int *singular_col);
+
+/* ---- batches ---- */
+void lusp_batch_opts_default(lusp_batch_opts *o);
+int lusp_batch_create(int nsys, lusp_pattern *const *pats, const lusp_batch_opts *opts,
+                      lusp_batch **out);
+void lusp_batch_destroy(lusp_batch *b);
+/* Device buffers of system sys (valid for the batch lifetime). */
+int lusp_batch_device_ptrs(lusp_batch *b, int sys, double **d_vals, double **d_rhs, double **d_x);
+/* Host <-> device copies for all systems, concatenated in system order
+ * (values: nnz_a of each system; rhs / x: n of each system). */
+int lusp_batch_upload(lusp_batch *b, const double *vals, const double *rhs, void *stream);
+int lusp_batch_download(lusp_batch *b, double *x, void *stream);
+/* One persistent launch: refactor and/or solve every system. */
+int lusp_batch_run(lusp_batch *b, int what, void *stream);
+/* Same as lusp_batch_run, replayed from a CUDA graph captured on first use
+ * (one graph per (what, stream)). */
+int lusp_batch_run_graph(lusp_batch *b, int what, void *stream);
+/* Copy per-system statistics to the host (synchronizes the stream). */
+int lusp_batch_stats(lusp_batch *b, lusp_sys_stats *out, void *stream);
+/* Merged factor values of one system (cap entries; float for LUSP_MIXED,
+ * double for LUSP_FP64), synchronizing copy. */
+int lusp_batch_factor_values(lusp_batch *b, int sys, void *out, void *stream);
+/* Device-to-device copy of all input values from src to dst (both batches
+ * must hold the same patterns in the same order). */
+int lusp_batch_copy_values(lusp_batch *dst, const lusp_batch *src, void *stream);
+/* Device pointer to the merged factor values of one system. */
+int lusp_batch_factor_device_ptr(lusp_batch *b, int sys, void **d_values);
+/* Update max_outer, rtol, inner_rel, stag_ratio and pivot_tol (prec,
+ * krylov and the launch shape are fixed at creation). */
+int lusp_batch_set_params(lusp_batch *b, const lusp_batch_opts *opts);
+/* Kernel launches issued by the last lusp_batch_run (for accounting). */
+int lusp_batch_launch_count(const lusp_batch *b);
+
+/* ---- SELL-C-sigma SpMV (standalone, whole GPU) ---- */
+typedef struct lusp_sell lusp_sell;
+/* Build from a 0-based CSR: C in {8,16,32}, sigma >= C (row sort window),
+ * value storage 0 = fp64, 1 = fp32, 2 = fp16 with Ruiz scaling (values are
+ * stored as D_r A D_c in fp16, y = D_r^-1 (S (D_c^-1 x)); creation fails
+ * with LUSP_EARG when a scaled value is outside the fp16 normal range). */
+int lusp_sell_create(int n, const int *rowptr, const int *colidx, const double *vals,
+                     int C, int sigma, int value_kind, lusp_sell **out);
+void lusp_sell_destroy(lusp_sell *s);
+/* y = A x, fp64 accumulation; d_x, d_y device pointers of n doubles. */
+int lusp_sell_spmv(const lusp_sell *s, const double *d_x, double *d_y, void *stream);
+int lusp_sell_info(const lusp_sell *s, long *stored, long *nnz, double *fp16_scaled_min,
+                   double *fp16_scaled_max);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LUSPICE_B200_H */

@@ -1,0 +1,164 @@
+"""ctypes bindings of libluspice_b200.so (every symbol the include/*.h headers
+declare as extern "C").  Loading fails loudly when the library is missing:
+there is no Python or CPU fallback for any operation."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libluspice_b200.so"
+
+c_int_p = C.POINTER(C.c_int)
+c_long_p = C.POINTER(C.c_long)
+c_double_p = C.POINTER(C.c_double)
+c_void_pp = C.POINTER(C.c_void_p)
+
+
+class PatternInfo(C.Structure):
+    _fields_ = [("n", C.c_int), ("nnz_a", C.c_int), ("lnnz", C.c_long), ("unnz", C.c_long),
+                ("cap", C.c_long), ("ncol_levels", C.c_int), ("nfwd_levels", C.c_int),
+                ("nbwd_levels", C.c_int), ("max_col", C.c_int), ("nslices", C.c_int),
+                ("sell_total", C.c_int), ("flops", C.c_long), ("gathered", C.c_long),
+                ("hash", C.c_ulonglong), ("device_bytes", C.c_size_t), ("singular_col", C.c_int)]
+
+
+class SysStats(C.Structure):
+    _fields_ = [("min_abs_pivot", C.c_double), ("min_pivot_ratio", C.c_double),
+                ("max_abs_u", C.c_double), ("res", C.c_double * 16), ("nres", C.c_int),
+                ("inner_iters", C.c_int), ("outer_iters", C.c_int), ("status", C.c_int),
+                ("singular_col", C.c_int), ("pad_", C.c_int)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("prec", C.c_int), ("krylov", C.c_int), ("max_outer", C.c_int),
+                ("rtol", C.c_double), ("inner_rel", C.c_double), ("stag_ratio", C.c_double),
+                ("pivot_tol", C.c_double), ("block_threads", C.c_int), ("ctas_per_sm", C.c_int)]
+
+
+class DshLuStatic(C.Structure):
+    """dsh_lu_static (lu_static.h), field for field."""
+    _fields_ = [("n", C.c_int), ("cnnz", C.c_long), ("lnnz", C.c_long), ("unnz", C.c_long),
+                ("cap", C.c_long), ("Ap", c_int_p), ("Ai", c_int_p), ("Ax", C.c_void_p),
+                ("P", c_int_p), ("Q", c_int_p), ("min_diag_U", C.c_double),
+                ("pivot_growth", C.c_double), ("dev_allocated", C.c_int),
+                ("factor_cache", C.c_void_p), ("pin", C.c_double)]
+
+
+class CSRMatrix(C.Structure):
+    _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("rowptr", c_int_p),
+                ("colidx", c_int_p), ("values", c_double_p)]
+
+
+class DshMatrixInfo(C.Structure):
+    _fields_ = [("n", C.c_int), ("nnz", C.c_long), ("avg_rowlen", C.c_double),
+                ("max_rowlen", C.c_double), ("p50_rowlen", C.c_double), ("row_skew", C.c_double),
+                ("kappa_ruiz", C.c_double), ("kappa_est", C.c_double),
+                ("dyn_range_log10", C.c_double), ("singular_flag", C.c_int)]
+
+
+class DshConfig(C.Structure):
+    _fields_ = [("spmv_format", C.c_int), ("sigma", C.c_int), ("use_ruiz", C.c_int),
+                ("use_shift", C.c_int), ("shift", C.c_double), ("factor_prec", C.c_int),
+                ("ir_outer", C.c_int), ("ir_inner", C.c_int), ("ir_rtol", C.c_double),
+                ("mp_path", C.c_int), ("pre_ruiz_hint", C.c_int), ("fp16_candidate", C.c_int)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    # luspice_b200.h
+    "lusp_last_error": (C.c_char_p, []),
+    "lusp_version": (C.c_char_p, []),
+    "lusp_device_count": (C.c_int, []),
+    "lusp_pattern_create": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, c_void_pp]),
+    "lusp_pattern_destroy": (None, [C.c_void_p]),
+    "lusp_pattern_get_info": (C.c_int, [C.c_void_p, C.POINTER(PatternInfo)]),
+    "lusp_pattern_get_perm": (C.c_int, [C.c_void_p, c_int_p, c_int_p]),
+    "lusp_pattern_get_structure": (C.c_int, [C.c_void_p, c_int_p, c_int_p, c_int_p]),
+    "lusp_pattern_get_levels": (C.c_int, [C.c_void_p, c_int_p]),
+    "lusp_colamd": (C.c_int, [C.c_int, C.c_int, c_int_p, c_int_p, C.c_double, C.c_double, c_int_p]),
+    "lusp_pivot_factor": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, C.c_double,
+                                    c_int_p, c_int_p, c_int_p, c_double_p, C.c_long,
+                                    c_int_p, c_int_p, c_double_p, C.c_long,
+                                    c_long_p, c_long_p, c_int_p]),
+    "lusp_batch_opts_default": (None, [C.POINTER(BatchOpts)]),
+    "lusp_batch_create": (C.c_int, [C.c_int, c_void_pp, C.POINTER(BatchOpts), c_void_pp]),
+    "lusp_batch_destroy": (None, [C.c_void_p]),
+    "lusp_batch_device_ptrs": (C.c_int, [C.c_void_p, C.c_int, c_void_pp, c_void_pp, c_void_pp]),
+    "lusp_batch_upload": (C.c_int, [C.c_void_p, c_double_p, c_double_p, C.c_void_p]),
+    "lusp_batch_download": (C.c_int, [C.c_void_p, c_double_p, C.c_void_p]),
+    "lusp_batch_run": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "lusp_batch_run_graph": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "lusp_batch_stats": (C.c_int, [C.c_void_p, C.POINTER(SysStats), C.c_void_p]),
+    "lusp_batch_factor_values": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "lusp_batch_copy_values": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "lusp_batch_factor_device_ptr": (C.c_int, [C.c_void_p, C.c_int, c_void_pp]),
+    "lusp_batch_set_params": (C.c_int, [C.c_void_p, C.POINTER(BatchOpts)]),
+    "lusp_batch_launch_count": (C.c_int, [C.c_void_p]),
+    "lusp_sell_create": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, C.c_int, C.c_int,
+                                   C.c_int, c_void_pp]),
+    "lusp_sell_destroy": (None, [C.c_void_p]),
+    "lusp_sell_spmv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "lusp_sell_info": (C.c_int, [C.c_void_p, c_long_p, c_long_p, c_double_p, c_double_p]),
+    # lu_gpu_par.h (C-ABI launchers)
+    "lusp_lu_factor_par_launch": (C.c_int, [C.c_int] + [C.c_void_p] * 7 + [C.c_long]
+                                  + [C.c_void_p] * 3 + [C.c_long] + [C.c_void_p] * 7),
+    "lusp_trisolve_par_launch": (C.c_int, [C.c_int] + [C.c_void_p] * 13),
+    # lu_static.h
+    "dsh_symbolic": (C.c_int, [C.c_int, C.c_long, c_int_p, c_int_p, c_int_p, C.POINTER(DshLuStatic)]),
+    "dsh_numeric": (C.c_int, [C.POINTER(DshLuStatic), c_int_p, c_int_p, c_double_p, C.c_int]),
+    "dsh_trisolve": (C.c_int, [C.POINTER(DshLuStatic), c_double_p, c_double_p]),
+    "dsh_gmres_ir": (C.c_int, [C.POINTER(DshLuStatic), c_double_p, c_double_p, C.c_int, C.c_int,
+                               C.c_double, c_double_p, c_int_p]),
+    "dsh_lu_static_init": (C.c_int, [C.POINTER(DshLuStatic)]),
+    "dsh_lu_static_alloc": (C.c_int, [C.POINTER(DshLuStatic)]),
+    "dsh_lu_static_free": (None, [C.POINTER(DshLuStatic)]),
+    "dsh_lu_status_str": (C.c_char_p, [C.c_int]),
+    "dsh_symbolic_count": (C.c_long, []),
+    # level.h
+    "dsh_level_compute": (C.c_int, [C.c_int, c_int_p, c_int_p, c_int_p, c_int_p]),
+    "dsh_level_hist": (C.c_int, [C.c_int, c_int_p, C.c_int, c_int_p]),
+    # spmv.h
+    "read_s0_to_csr": (C.c_int, [C.c_char_p, C.POINTER(CSRMatrix)]),
+    "csr_free": (None, [C.POINTER(CSRMatrix)]),
+    "read_rhs": (C.c_int, [C.c_char_p, C.c_int, c_double_p]),
+    "spmv_host": (C.c_int, [C.POINTER(CSRMatrix), c_double_p, c_double_p, c_double_p]),
+    "csr_alloc_device": (C.c_int, [C.POINTER(CSRMatrix), C.POINTER(c_int_p), C.POINTER(c_int_p),
+                                   C.POINTER(c_double_p)]),
+    "spmv_launch": (None, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                           C.c_void_p]),
+    # selector.h
+    "dsh_matrix_analyze": (None, [C.c_int, C.c_long, c_int_p, C.POINTER(DshMatrixInfo)]),
+    "dsh_format_select": (None, [C.POINTER(DshMatrixInfo), C.POINTER(DshConfig)]),
+    "dsh_fmt_name": (C.c_char_p, [C.c_int]),
+    "dsh_mp_initial": (None, [C.POINTER(DshMatrixInfo), C.POINTER(DshConfig)]),
+    "dsh_mp_escalate": (C.c_int, [C.c_int]),
+    "dsh_mp_name": (C.c_char_p, [C.c_int]),
+}
+
+_lib = None
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load the library once and attach signatures.  Raises when it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build it with `python -m luspice_b200.build` "
+                           "(the package has no fallback implementation)")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def ptr(a, ctype):
+    """ctypes pointer to a contiguous numpy array (or None)."""
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))

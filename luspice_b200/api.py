@@ -1,0 +1,264 @@
+"""Python host wrapper over the lusp_* C-ABI (luspice_b200.h).
+
+Patterns, batches and the standalone SELL SpMV as Python objects; every call
+goes through libluspice_b200.so.  Streams are raw cudaStream_t handles
+(e.g. torch.cuda.Stream().cuda_stream) or None for the default stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+MIXED, FP64 = 0, 1
+RUN_REFACTOR, RUN_SOLVE, RUN_BOTH, RUN_DIRECT = 1, 2, 3, 4
+
+ST_SINGULAR, ST_PIVOT_WEAK, ST_STAGNATED, ST_NOT_CONVERGED = 1, 2, 4, 8
+ST_NONFINITE, ST_WAIT_TIMEOUT, ST_CAPACITY, ST_ESCALATED = 16, 32, 64, 128
+ST_FAIL_MASK = ST_SINGULAR | ST_STAGNATED | ST_NOT_CONVERGED | ST_NONFINITE | ST_WAIT_TIMEOUT | ST_CAPACITY
+
+
+class LuspError(RuntimeError):
+    def __init__(self, rc: int, what: str):
+        lib = L.load()
+        msg = lib.lusp_last_error().decode(errors="replace")
+        super().__init__(f"{what}: rc={rc} {msg}")
+        self.rc = rc
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise LuspError(rc, what)
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _stream(s) -> C.c_void_p:
+    if s is None:
+        return None
+    if hasattr(s, "cuda_stream"):
+        return C.c_void_p(s.cuda_stream)
+    return C.c_void_p(int(s))
+
+
+class Pattern:
+    """Host analysis + device-resident static layout of one sparsity pattern."""
+
+    def __init__(self, n: int, Ap, Ai, Ax, q=None):
+        lib = L.load()
+        self.n = int(n)
+        self._Ap, self._Ai, self._Ax = _i32(Ap), _i32(Ai), _f64(Ax)
+        qq = None if q is None else _i32(q)
+        h = C.c_void_p()
+        rc = lib.lusp_pattern_create(self.n, L.ptr(self._Ap, C.c_int), L.ptr(self._Ai, C.c_int),
+                                     L.ptr(self._Ax, C.c_double), L.ptr(qq, C.c_int), C.byref(h))
+        _check(rc, "lusp_pattern_create")
+        self.handle = h
+        info = L.PatternInfo()
+        _check(lib.lusp_pattern_get_info(h, C.byref(info)), "lusp_pattern_get_info")
+        self.info = {k: getattr(info, k) for k, _ in L.PatternInfo._fields_}
+
+    @classmethod
+    def from_matrix(cls, m, q=None, values=None):
+        return cls(m.n, m.Ap, m.Ai, m.Ax if values is None else values, q)
+
+    def perm(self) -> tuple[np.ndarray, np.ndarray]:
+        pinv = np.empty(self.n, np.int32)
+        q = np.empty(self.n, np.int32)
+        _check(L.load().lusp_pattern_get_perm(self.handle, L.ptr(pinv, C.c_int), L.ptr(q, C.c_int)), "perm")
+        return pinv, q
+
+    def structure(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        cp = np.empty(self.n + 1, np.int32)
+        ri = np.empty(self.info["cap"], np.int32)
+        dg = np.empty(self.n, np.int32)
+        _check(L.load().lusp_pattern_get_structure(self.handle, L.ptr(cp, C.c_int), L.ptr(ri, C.c_int),
+                                                   L.ptr(dg, C.c_int)), "structure")
+        return cp, ri, dg
+
+    def levels(self) -> np.ndarray:
+        lv = np.empty(self.n, np.int32)
+        _check(L.load().lusp_pattern_get_levels(self.handle, L.ptr(lv, C.c_int)), "levels")
+        return lv
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            L.load().lusp_pattern_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def default_opts() -> L.BatchOpts:
+    o = L.BatchOpts()
+    L.load().lusp_batch_opts_default(C.byref(o))
+    return o
+
+
+class Batch:
+    """N systems refactored and solved by one persistent launch."""
+
+    def __init__(self, patterns: Sequence[Pattern], prec: int = MIXED, **opts):
+        lib = L.load()
+        o = default_opts()
+        o.prec = prec
+        for k, v in opts.items():
+            if not hasattr(o, k):
+                raise TypeError(f"unknown batch option {k}")
+            setattr(o, k, v)
+        self.opts = o
+        self.patterns = list(patterns)
+        arr = (C.c_void_p * len(self.patterns))(*[p.handle for p in self.patterns])
+        h = C.c_void_p()
+        _check(lib.lusp_batch_create(len(self.patterns), arr, C.byref(o), C.byref(h)), "lusp_batch_create")
+        self.handle = h
+        self.nsys = len(self.patterns)
+        self.sizes = np.array([p.n for p in self.patterns], dtype=np.int64)
+        self.nnzs = np.array([p.info["nnz_a"] for p in self.patterns], dtype=np.int64)
+
+    def set_params(self, **opts) -> None:
+        for k, v in opts.items():
+            setattr(self.opts, k, v)
+        _check(L.load().lusp_batch_set_params(self.handle, C.byref(self.opts)), "set_params")
+
+    def upload(self, values=None, rhs=None, stream=None) -> None:
+        v = None if values is None else _f64(np.concatenate([np.ravel(a) for a in values])
+                                             if isinstance(values, (list, tuple)) else np.ravel(values))
+        b = None if rhs is None else _f64(np.concatenate([np.ravel(a) for a in rhs])
+                                          if isinstance(rhs, (list, tuple)) else np.ravel(rhs))
+        if v is not None and v.size != self.nnzs.sum():
+            raise ValueError("values size mismatch")
+        if b is not None and b.size != self.sizes.sum():
+            raise ValueError("rhs size mismatch")
+        self._keep = (v, b)  # host buffers must outlive asynchronous copies
+        _check(L.load().lusp_batch_upload(self.handle, L.ptr(v, C.c_double), L.ptr(b, C.c_double),
+                                          _stream(stream)), "upload")
+
+    def run(self, what: int = RUN_BOTH, stream=None, graph: bool = False) -> None:
+        lib = L.load()
+        fn = lib.lusp_batch_run_graph if graph else lib.lusp_batch_run
+        _check(fn(self.handle, what, _stream(stream)), "run")
+
+    def download(self, out: np.ndarray | None = None, stream=None) -> np.ndarray:
+        x = np.empty(int(self.sizes.sum())) if out is None else out
+        _check(L.load().lusp_batch_download(self.handle, L.ptr(x, C.c_double), _stream(stream)), "download")
+        return x
+
+    def split(self, flat: np.ndarray) -> list[np.ndarray]:
+        return np.split(flat, np.cumsum(self.sizes)[:-1])
+
+    def stats(self, stream=None) -> list[dict]:
+        arr = (L.SysStats * self.nsys)()
+        _check(L.load().lusp_batch_stats(self.handle, arr, _stream(stream)), "stats")
+        out = []
+        for s in arr:
+            d = {k: getattr(s, k) for k, _ in L.SysStats._fields_ if k not in ("res", "pad_")}
+            d["res"] = [s.res[i] for i in range(min(max(s.nres, 0), 16))]
+            out.append(d)
+        return out
+
+    def factor_values(self, sys: int, stream=None) -> np.ndarray:
+        cap = self.patterns[sys].info["cap"]
+        out = np.empty(cap, np.float32 if self.opts.prec == MIXED else np.float64)
+        _check(L.load().lusp_batch_factor_values(self.handle, sys, out.ctypes.data_as(C.c_void_p),
+                                                 _stream(stream)), "factor_values")
+        return out
+
+    def device_ptrs(self, sys: int) -> tuple[int, int, int]:
+        a, b, x = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        _check(L.load().lusp_batch_device_ptrs(self.handle, sys, C.byref(a), C.byref(b), C.byref(x)), "ptrs")
+        return a.value, b.value, x.value
+
+    def launch_count(self) -> int:
+        return L.load().lusp_batch_launch_count(self.handle)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            L.load().lusp_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Sell:
+    """Standalone SELL-C-sigma SpMV over a 0-based CSR matrix."""
+
+    KINDS = {"fp64": 0, "fp32": 1, "fp16": 2}
+
+    def __init__(self, n, rowptr, colidx, vals, C_: int = 32, sigma: int = 256, kind: str = "fp32"):
+        lib = L.load()
+        self.n = int(n)
+        rp, ci, v = _i32(rowptr), _i32(colidx), _f64(vals)
+        h = C.c_void_p()
+        _check(lib.lusp_sell_create(self.n, L.ptr(rp, C.c_int), L.ptr(ci, C.c_int), L.ptr(v, C.c_double),
+                                    C_, sigma, self.KINDS[kind], C.byref(h)), "lusp_sell_create")
+        self.handle = h
+        st, nz, mn, mx = C.c_long(), C.c_long(), C.c_double(), C.c_double()
+        lib.lusp_sell_info(h, C.byref(st), C.byref(nz), C.byref(mn), C.byref(mx))
+        self.stored, self.nnz, self.scaled_min, self.scaled_max = st.value, nz.value, mn.value, mx.value
+
+    def spmv(self, d_x: int, d_y: int, stream=None) -> None:
+        _check(L.load().lusp_sell_spmv(self.handle, C.c_void_p(d_x), C.c_void_p(d_y), _stream(stream)), "spmv")
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            L.load().lusp_sell_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def colamd(n: int, Ap, Ai, knob_row: float = 0.0, knob_col: float = 0.0) -> np.ndarray:
+    Ap, Ai = _i32(Ap), _i32(Ai)
+    q = np.empty(n, np.int32)
+    _check(L.load().lusp_colamd(n, n, L.ptr(Ap, C.c_int), L.ptr(Ai, C.c_int), knob_row, knob_col,
+                                L.ptr(q, C.c_int)), "lusp_colamd")
+    return q
+
+
+def pivot_factor(n: int, Ap, Ai, Ax, q=None, tol: float = 1.0) -> dict:
+    """Host pivoting LU in splu layout (the analysis step of pattern creation)."""
+    lib = L.load()
+    Ap, Ai, Ax = _i32(Ap), _i32(Ai), _f64(Ax)
+    qq = None if q is None else _i32(q)
+    ln, un, sc = C.c_long(), C.c_long(), C.c_int()
+    pinv = np.empty(n, np.int32)
+    Lp = np.empty(n + 1, np.int32)
+    Up = np.empty(n + 1, np.int32)
+    args = lambda Li, Lx, Ui, Ux, cap: (n, L.ptr(Ap, C.c_int), L.ptr(Ai, C.c_int), L.ptr(Ax, C.c_double),
+                                        L.ptr(qq, C.c_int), tol, L.ptr(pinv, C.c_int), L.ptr(Lp, C.c_int),
+                                        L.ptr(Li, C.c_int), L.ptr(Lx, C.c_double), cap, L.ptr(Up, C.c_int),
+                                        L.ptr(Ui, C.c_int), L.ptr(Ux, C.c_double), cap, C.byref(ln),
+                                        C.byref(un), C.byref(sc))
+    rc = lib.lusp_pivot_factor(*args(None, None, None, None, 0))
+    if rc == 1:
+        return {"singular_col": sc.value}
+    if rc not in (0, 2):
+        _check(rc, "lusp_pivot_factor")
+    cap = max(ln.value, un.value)
+    Li, Ui = np.empty(cap, np.int32), np.empty(cap, np.int32)
+    Lx, Ux = np.empty(cap), np.empty(cap)
+    _check(lib.lusp_pivot_factor(*args(Li, Lx, Ui, Ux, cap)), "lusp_pivot_factor")
+    return {"singular_col": -1, "pinv": pinv, "Lp": Lp, "Li": Li[:ln.value], "Lx": Lx[:ln.value],
+            "Up": Up, "Ui": Ui[:un.value], "Ux": Ux[:un.value], "lnnz": ln.value, "unnz": un.value}

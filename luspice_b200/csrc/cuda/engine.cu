@@ -1,0 +1,387 @@
+// Batched refactor-and-solve engine: pattern objects (host analysis + the
+// device-resident static layout), batches of systems, the persistent kernel
+// and the lusp_* C-ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "luspice_b200.h"
+#include "../host/lusp_host.h"
+#include "engine_internal.h"
+#include "phases.cuh"
+
+namespace lusp {
+
+// ---------------------------------------------------------------------------
+// Error reporting
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+const char* last_error_cstr() { return g_last_error.c_str(); }
+
+void set_error(const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return LUSP_ECUDA;
+}
+
+// ---------------------------------------------------------------------------
+// The persistent kernel: every CTA takes systems from the device work queue
+// until it is empty; for each one it runs the requested phases.
+// ---------------------------------------------------------------------------
+template <typename VT, typename AT>
+__global__ void __launch_bounds__(512)
+batch_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan,
+             SolveParams prm, int what, int direct) {
+    extern __shared__ __align__(16) char smem[];
+    __shared__ int s_task;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_task = atomicAdd(queue, 1);
+        __syncthreads();
+        const int t = s_task;
+        if (t >= nsys) break;
+        const SysDev S = sys[t];
+        if (what & LUSP_RUN_REFACTOR) refactor_phase<VT>(S, plan, smem, prm);
+        if (what & LUSP_RUN_SOLVE) {
+            if (direct) direct_phase<VT>(S, plan, smem);
+            else gmres_phase<VT, AT>(S, plan, smem, prm);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Patterns
+// ---------------------------------------------------------------------------
+static int upload_ints(const std::vector<int>& v, int* dst, cudaStream_t st) {
+    if (v.empty()) return 0;
+    cudaError_t e = cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "pattern upload");
+}
+
+int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const int* q_in,
+                  PatternObj** out) {
+    *out = nullptr;
+    if (n <= 0 || !Ap || !Ai || !Ax) { set_error("pattern_create: bad arguments"); return LUSP_EARG; }
+    const int nnz = Ap[n];
+    if (Ap[0] != 0 || nnz < 0) { set_error("pattern_create: bad column pointers"); return LUSP_EARG; }
+    for (int c = 0; c < n; c++)
+        if (Ap[c + 1] < Ap[c]) { set_error("pattern_create: column pointers decrease at %d", c); return LUSP_EARG; }
+    for (int p = 0; p < nnz; p++)
+        if (Ai[p] < 0 || Ai[p] >= n) { set_error("pattern_create: row index out of range at %d", p); return LUSP_EARG; }
+    if (q_in) {
+        std::vector<char> seen(n, 0);
+        for (int k = 0; k < n; k++) {
+            if (q_in[k] < 0 || q_in[k] >= n || seen[q_in[k]]) { set_error("pattern_create: q is not a permutation"); return LUSP_EARG; }
+            seen[q_in[k]] = 1;
+        }
+    }
+    // Column-sorted, duplicate-summed copy for the analysis.
+    std::vector<int> Bp(n + 1, 0), Bi;
+    std::vector<double> Bx;
+    Bi.reserve(nnz);
+    Bx.reserve(nnz);
+    {
+        std::vector<std::pair<int, double>> col;
+        for (int c = 0; c < n; c++) {
+            col.clear();
+            for (int p = Ap[c]; p < Ap[c + 1]; p++) col.emplace_back(Ai[p], Ax[p]);
+            std::stable_sort(col.begin(), col.end(),
+                             [](const std::pair<int, double>& a, const std::pair<int, double>& b) { return a.first < b.first; });
+            for (size_t t = 0; t < col.size(); t++) {
+                if (t > 0 && col[t].first == col[t - 1].first) Bx.back() += col[t].second;
+                else { Bi.push_back(col[t].first); Bx.push_back(col[t].second); }
+            }
+            Bp[c + 1] = (int)Bi.size();
+        }
+    }
+    std::vector<int> q(n);
+    if (q_in) {
+        std::copy(q_in, q_in + n, q.begin());
+    } else if (colamd_order(n, n, Bp.data(), Bi.data(), 0.0, 0.0, q.data()) != 0) {
+        set_error("pattern_create: COLAMD failed");
+        return LUSP_EARG;
+    }
+    PivotFactor F;
+    const int sc = pivot_factor(n, Bp.data(), Bi.data(), Bx.data(), q.data(), 1.0, F);
+    if (sc >= 0) {
+        set_error("pattern_create: singular at column %d", sc);
+        return LUSP_ESINGULAR;
+    }
+    PatternObj* P = new PatternObj();
+    build_static_pattern(n, Ap, Ai, q.data(), F, 256, P->S);
+    const StaticPattern& S = P->S;
+
+    // One device block for every int array of the layout.
+    const std::vector<int>* arrays[] = {&S.cp, &S.ri, &S.dg, &S.col_order, &S.a_ptr, &S.a_src, &S.a_dst,
+                                        &S.lrp, &S.lci, &S.urp, &S.uci, &S.slot_dst, &S.fwd_order,
+                                        &S.bwd_order, &S.sell_ptr, &S.sell_col, &S.sell_src,
+                                        &S.sell_perm, &S.rowat, &S.q};
+    const int narr = (int)(sizeof(arrays) / sizeof(arrays[0]));
+    std::vector<size_t> off(narr + 1, 0);
+    for (int a = 0; a < narr; a++) off[a + 1] = off[a] + ((arrays[a]->size() + 31) & ~(size_t)31);
+    int* blk = nullptr;
+    cudaError_t e = cudaMalloc(&blk, std::max<size_t>(off[narr], 32) * sizeof(int));
+    if (e != cudaSuccess) { delete P; return cuda_fail(e, "pattern device alloc"); }
+    P->d_block = blk;
+    P->bytes = off[narr] * sizeof(int) + sizeof(PatternDev);
+    for (int a = 0; a < narr; a++) {
+        int rc = upload_ints(*arrays[a], blk + off[a], 0);
+        if (rc) { pattern_free(P); return rc; }
+    }
+    PatternDev& D = P->desc;
+    D.n = n;
+    D.nnz_a = S.nnz_a;
+    D.cap = (int)S.cap;
+    D.max_col = S.max_col;
+    D.nslices = S.nslices;
+    D.sell_total = S.sell_ptr.empty() ? 0 : S.sell_ptr.back();
+    D.nnz_l = (int)S.lci.size();
+    D.nnz_u = (int)S.uci.size();
+    int idx = 0;
+    D.cp = blk + off[idx++];
+    D.ri = blk + off[idx++];
+    D.dg = blk + off[idx++];
+    D.col_order = blk + off[idx++];
+    D.a_ptr = blk + off[idx++];
+    D.a_src = blk + off[idx++];
+    D.a_dst = blk + off[idx++];
+    D.lrp = blk + off[idx++];
+    D.lci = blk + off[idx++];
+    D.urp = blk + off[idx++];
+    D.uci = blk + off[idx++];
+    D.slot_dst = blk + off[idx++];
+    D.fwd_order = blk + off[idx++];
+    D.bwd_order = blk + off[idx++];
+    D.sell_ptr = blk + off[idx++];
+    D.sell_col = blk + off[idx++];
+    D.sell_src = blk + off[idx++];
+    D.sell_perm = blk + off[idx++];
+    D.rowat = blk + off[idx++];
+    D.q = blk + off[idx++];
+    e = cudaMalloc(&P->d_desc, sizeof(PatternDev));
+    if (e != cudaSuccess) { pattern_free(P); return cuda_fail(e, "pattern descriptor alloc"); }
+    e = cudaMemcpy(P->d_desc, &D, sizeof(PatternDev), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { pattern_free(P); return cuda_fail(e, "pattern descriptor upload"); }
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) { pattern_free(P); return cuda_fail(e, "pattern upload sync"); }
+    *out = P;
+    return LUSP_OK;
+}
+
+void pattern_free(PatternObj* P) {
+    if (!P) return;
+    if (P->d_block) cudaFree(P->d_block);
+    if (P->d_desc) cudaFree(P->d_desc);
+    delete P;
+}
+
+// ---------------------------------------------------------------------------
+// Batches
+// ---------------------------------------------------------------------------
+static int sm_count() {
+    static int cached = 0;
+    if (!cached) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) cached = 148;
+    }
+    return cached;
+}
+
+static size_t smem_fixed(int nwords) { return 64 + (((size_t)nwords * 4 + 15) & ~(size_t)15) + 40 * sizeof(double); }
+
+void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm, int m, SmemPlan& plan) {
+    int nmax = 1, colmax = 1;
+    for (auto* p : pats) {
+        nmax = std::max(nmax, p->S.n);
+        colmax = std::max(colmax, p->S.max_col);
+    }
+    const size_t limit = 227 * 1024;
+    size_t budget = 228 * 1024 / std::max(1, ctas_per_sm);
+    budget = budget > 1024 ? budget - 1024 : budget;
+    budget = std::min(budget, limit);
+    plan.nwords = (nmax + 31) / 32;
+    plan.m = m;
+    const size_t fixed = smem_fixed(plan.nwords);
+    const int nw = block / 32;
+    const size_t hbytes = ((size_t)(m + 1) * m + 6 * (size_t)(m + 1)) * sizeof(double);
+    size_t avail = budget > fixed + hbytes ? budget - fixed - hbytes : 0;
+    // Solve vector in shared memory when it fits.
+    plan.ycap = ((size_t)nmax * 8 <= avail) ? nmax : 0;
+    // Refactor work area per warp.
+    size_t ravail = budget > fixed ? budget - fixed : 0;
+    int wcap = (int)std::min<size_t>((size_t)colmax, ravail / ((size_t)nw * 12));
+    plan.wcap = std::max(wcap, 0);
+    const size_t solve_bytes = (size_t)plan.ycap * 8 + hbytes;
+    const size_t ref_bytes = (size_t)plan.wcap * nw * 12;
+    plan.bytes = fixed + std::max(solve_bytes, ref_bytes);
+}
+
+template <typename VT, typename AT>
+static int launch_typed(BatchObj* B, int what, cudaStream_t st) {
+    auto kern = batch_kernel<VT, AT>;
+    // Raise the dynamic shared-memory limit once per size (not a stream
+    // operation, so it stays out of captured graphs after the first call).
+    static std::mutex mu;
+    static size_t granted = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (B->plan.bytes > granted) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->plan.bytes);
+            if (e != cudaSuccess) return cuda_fail(e, "kernel smem attribute");
+            granted = B->plan.bytes;
+        }
+    }
+    cudaError_t e = cudaMemsetAsync(B->d_queue, 0, sizeof(int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "queue reset");
+    const int direct = (B->prec == LUSP_FP64 || (what & LUSP_RUN_DIRECT)) ? 1 : 0;
+    kern<<<B->grid, B->block, B->plan.bytes, st>>>(B->d_sys, B->nsys, B->d_queue, B->plan, B->prm,
+                                                  what & 3, direct);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "batch kernel launch");
+    B->launches = 1;
+    return LUSP_OK;
+}
+
+int batch_launch(BatchObj* B, int what, cudaStream_t st) {
+    if (B->prec == LUSP_FP64) return launch_typed<double, double>(B, what, st);
+    return launch_typed<float, float>(B, what, st);
+}
+
+int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, BatchObj** out) {
+    *out = nullptr;
+    if (nsys <= 0 || !pats || !o) { set_error("batch_create: bad arguments"); return LUSP_EARG; }
+    for (int s = 0; s < nsys; s++)
+        if (!pats[s]) { set_error("batch_create: null pattern %d", s); return LUSP_EARG; }
+    if (o->prec != LUSP_MIXED && o->prec != LUSP_FP64) { set_error("batch_create: bad prec"); return LUSP_EARG; }
+    if (o->krylov < 1 || o->krylov > kMaxKrylov) { set_error("batch_create: krylov must be 1..%d", kMaxKrylov); return LUSP_EARG; }
+    if (o->block_threads < 64 || o->block_threads > 512 || o->block_threads % 32) { set_error("batch_create: block_threads"); return LUSP_EARG; }
+    BatchObj* B = new BatchObj();
+    B->nsys = nsys;
+    B->prec = o->prec;
+    B->opts = *o;
+    B->pats.assign(pats, pats + nsys);
+    B->block = o->block_threads;
+    B->prm.m = o->krylov;
+    B->prm.max_outer = std::max(0, o->max_outer);
+    B->prm.rtol = o->rtol;
+    B->prm.inner_rel = o->inner_rel;
+    B->prm.stag_ratio = o->stag_ratio;
+    B->prm.pivot_tol = o->pivot_tol;
+    make_plan(B->pats, B->block, o->ctas_per_sm, o->krylov, B->plan);
+
+    const size_t vs = B->prec == LUSP_FP64 ? 8 : 4;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    // Inputs and outputs of all systems are contiguous (values, rhs, x) so a
+    // batch moves host<->device in one copy each; the rest is per system.
+    std::vector<size_t> base(nsys + 1, 0);
+    B->val_off.assign(nsys + 1, 0);
+    B->vec_off.assign(nsys + 1, 0);
+    for (int s = 0; s < nsys; s++) {
+        B->val_off[s + 1] = B->val_off[s] + B->pats[s]->S.nnz_a;
+        B->vec_off[s + 1] = B->vec_off[s] + B->pats[s]->S.n;
+    }
+    const size_t io_bytes = al(B->val_off[nsys] * 8) + 2 * al(B->vec_off[nsys] * 8);
+    base[0] = io_bytes;
+    for (int s = 0; s < nsys; s++) {
+        const StaticPattern& S = B->pats[s]->S;
+        const size_t n = S.n;
+        const size_t st = S.sell_ptr.back();
+        size_t b = 0;
+        b += al(S.cap * vs);                        // lu
+        b += al(S.lci.size() * vs);                 // lval
+        b += al(S.uci.size() * vs);                 // uval
+        b += al(n * vs);                            // udiag
+        b += al(st * 8) + al(st * 4);               // sell64, sell32
+        b += al(((size_t)o->krylov + 8) * n * 8);   // work
+        base[s + 1] = base[s] + b;
+    }
+    // Spill area for columns longer than the shared-memory work area.
+    int colmax = 0;
+    for (auto* p : B->pats) colmax = std::max(colmax, p->S.max_col);
+    int occ = 0;
+    cudaError_t e;
+    if (B->prec == LUSP_FP64) {
+        cudaFuncSetAttribute(batch_kernel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->plan.bytes);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel<double, double>, B->block, B->plan.bytes);
+    } else {
+        cudaFuncSetAttribute(batch_kernel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->plan.bytes);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel<float, float>, B->block, B->plan.bytes);
+    }
+    if (e != cudaSuccess) { delete B; return cuda_fail(e, "occupancy query"); }
+    if (occ < 1) { delete B; set_error("batch_create: kernel does not fit one SM (smem %zu)", B->plan.bytes); return LUSP_EARG; }
+    B->grid = std::min(nsys, occ * sm_count());
+    const size_t spill = colmax > B->plan.wcap ? al((size_t)B->grid * (B->block / 32) * colmax * 8) : 0;
+    const size_t total = base[nsys] + spill + al(sizeof(SysStats) * nsys) + al(sizeof(SysDev) * nsys) + 256;
+    char* blk = nullptr;
+    e = cudaMalloc(&blk, total);
+    if (e != cudaSuccess) { delete B; return cuda_fail(e, "batch device alloc"); }
+    B->d_block = blk;
+    B->bytes = total;
+    e = cudaMemset(blk, 0, total);
+    if (e != cudaSuccess) { batch_free(B); return cuda_fail(e, "batch memset"); }
+    char* stats_base = blk + base[nsys] + spill;
+    B->d_stats = (SysStats*)stats_base;
+    B->d_sys = (SysDev*)(stats_base + al(sizeof(SysStats) * nsys));
+    B->d_queue = (int*)((char*)B->d_sys + al(sizeof(SysDev) * nsys));
+    double* spill_ptr = spill ? (double*)(blk + base[nsys]) : nullptr;
+    B->d_vals = (double*)blk;
+    B->d_rhs = (double*)(blk + al(B->val_off[nsys] * 8));
+    B->d_x = (double*)(blk + al(B->val_off[nsys] * 8) + al(B->vec_off[nsys] * 8));
+    B->h_sys.resize(nsys);
+    for (int s = 0; s < nsys; s++) {
+        const StaticPattern& S = B->pats[s]->S;
+        const size_t n = S.n;
+        const size_t st = S.sell_ptr.back();
+        char* p = blk + base[s];
+        SysDev& D = B->h_sys[s];
+        D.pat = B->pats[s]->d_desc;
+        D.a_val = B->d_vals + B->val_off[s];
+        D.b = B->d_rhs + B->vec_off[s];
+        D.x = B->d_x + B->vec_off[s];
+        D.lu = p; p += al(S.cap * vs);
+        D.lval = p; p += al(S.lci.size() * vs);
+        D.uval = p; p += al(S.uci.size() * vs);
+        D.udiag = p; p += al(n * vs);
+        D.sell64 = (double*)p; p += al(st * 8);
+        D.sell32 = (float*)p; p += al(st * 4);
+        D.work = (double*)p; p += al(((size_t)o->krylov + 8) * n * 8);
+        D.scratch = spill_ptr;
+        D.stats = B->d_stats + s;
+    }
+    e = cudaMemcpy(B->d_sys, B->h_sys.data(), sizeof(SysDev) * nsys, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { batch_free(B); return cuda_fail(e, "batch descriptor upload"); }
+    *out = B;
+    return LUSP_OK;
+}
+
+void batch_free(BatchObj* B) {
+    if (!B) return;
+    for (auto& kv : B->graphs) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    }
+    if (B->d_block) cudaFree(B->d_block);
+    delete B;
+}
+
+}  // namespace lusp

@@ -1,0 +1,93 @@
+// Internal host-side declarations shared by the host analysis code and the
+// CUDA engine.  Nothing here crosses the public C-ABI.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace lusp {
+
+// Result of the pivoting fp64 factorization that fixes the row permutation
+// and the structural L/U pattern (CSparse cs_lu layout, as the reference's
+// splu.h:29-41 stores it).
+struct PivotFactor {
+    int n = 0;
+    int singular_col = -1;          // -1 ok, >= 0 first column with no pivot
+    std::vector<int> pinv;          // pinv[orig_row] = pivot position
+    std::vector<int> Lp, Li;        // L: unit diagonal first, Li = positions
+    std::vector<double> Lx;
+    std::vector<int> Up, Ui;        // U: diagonal last, Ui = positions
+    std::vector<double> Ux;
+};
+
+// fp64 left-looking LU with threshold partial pivoting on the q-permuted
+// CSC of A (A given with original row indices, rows in any order, no
+// duplicate entries within a column).  Bit-for-bit the decisions of the
+// reference (splu.h:151-206): same depth-first reach order, same update
+// order, same pivot tie-breaks.  Returns singular_col.
+int pivot_factor(int n, const int* Ap, const int* Ai, const double* Ax,
+                 const int* q, double tol, PivotFactor& F);
+
+// Static layout of one sparsity pattern on the device, in pivot-position
+// space.  Column k of the merged factor is slots [cp[k], cp[k+1]): the
+// rows j < k of U(:,k) ascending, the diagonal at slot dg[k], then the rows
+// i > k of L(:,k) ascending.
+struct StaticPattern {
+    int n = 0;
+    int nnz_a = 0;                  // entries of the input CSC
+    long lnnz = 0, unnz = 0;        // splu-convention counts
+    long cap = 0;                   // merged slots = lnnz + unnz - n
+    uint64_t hash = 0;              // FNV-1a of (n, Ap, Ai, q)
+
+    std::vector<int> q, invq;       // column order and its inverse
+    std::vector<int> pinv, rowat;   // row permutation and its inverse
+
+    std::vector<int> cp, ri, dg;    // merged columns
+
+    // Column schedule: level-sorted column order for the refactorization.
+    std::vector<int> col_level, col_order;
+    int ncol_levels = 0;
+
+    // Input values -> slots.  For column k, entries [a_ptr[k], a_ptr[k+1])
+    // give a_src (index into the input value array) and a_dst (slot offset
+    // inside column k), sorted by a_dst (duplicates adjacent).
+    std::vector<int> a_ptr, a_src, a_dst;
+
+    // Row-major copies for the triangular solves.
+    // L (strictly lower, unit diagonal implicit): rows by position.
+    std::vector<int> lrp, lci;      // lci: column positions, ascending
+    // U (strictly upper): rows by position, column positions ascending.
+    std::vector<int> urp, uci;
+    // slot -> destination: L slots -> index in L-CSR, U slots -> index in
+    // U-CSR, diagonal slot -> k.
+    std::vector<int> slot_dst;
+    std::vector<int> fwd_order, bwd_order;   // level-sorted row orders
+    int nfwd_levels = 0, nbwd_levels = 0;
+
+    // Depth-first critical path lengths (longest chain of dependencies).
+    // SELL-C-sigma copy of A in position space (C = 32): slice s covers
+    // sorted rows [32 s, 32 s + 32); entry (r, t) of slice s is at
+    // sell_ptr[s] + 32 t + r.  sell_perm[32 s + r] = row position (-1 pad),
+    // sell_col = column position, sell_src = input index (-1 pad).
+    int sell_sigma = 256;
+    int nslices = 0;
+    std::vector<int> sell_ptr, sell_col, sell_src, sell_perm;
+
+    int max_col = 0;                // longest merged column (slots)
+    long flops = 0;                 // multiply-adds of one refactorization
+    long gathered = 0;              // sum over deps of |L(:,j)| (entries)
+};
+
+// Build the static layout from a pivot factorization.  Ap/Ai is the same
+// CSC (original indices) the factorization consumed.
+void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
+                          const PivotFactor& F, int sell_sigma, StaticPattern& S);
+
+uint64_t pattern_hash(int n, const int* Ap, const int* Ai, const int* q);
+
+// Column approximate minimum degree ordering (our own implementation of the
+// published COLAMD algorithm).  dense_row / dense_col: knob values as in
+// COLAMD's knobs[0..1] (0 -> threshold 16).  Returns 0 on success.
+int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
+                 double knob_dense_row, double knob_dense_col, int* q_out);
+
+}  // namespace lusp

@@ -1,0 +1,411 @@
+// Host symbolic analysis: the pivoting fp64 factorization that fixes the row
+// permutation and the structural L/U pattern, and the static device layout
+// derived from it (merged columns, level schedules, row-major copies, value
+// scatter maps, SELL-C-sigma copy of A).
+//
+// Build with -ffp-contract=off: the pivot decisions compare values, and the
+// values must be computed with exactly the reference's operation sequence.
+#include "lusp_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace lusp {
+
+namespace {
+
+// Depth-first search from original row j over the graph of L (node v has
+// the edges L(:, pinv[v]) when v is pivoted).  Nodes are appended to
+// xi[--top] in finishing order, so xi[top..n) is a topological order.  The
+// stack lives in xi[0..head] and pstack; a node resumes its edge scan where
+// it left off.  Same traversal as splu.h:77-106 (CSparse cs_dfs), which the
+// pivot tie-breaks depend on.
+int dfs_from(int j, const int* Lp, const int* Li, int top, int* xi,
+             int* pstack, const int* pinv, unsigned char* mark) {
+    int head = 0;
+    xi[0] = j;
+    while (head >= 0) {
+        const int v = xi[head];
+        const int col = pinv[v];
+        if (!mark[v]) {
+            mark[v] = 1;
+            pstack[head] = (col < 0) ? 0 : Lp[col];
+        }
+        const int pend = (col < 0) ? 0 : Lp[col + 1];
+        int pushed = 0;
+        for (int p = pstack[head]; p < pend; p++) {
+            const int w = Li[p];
+            if (mark[w]) continue;
+            pstack[head] = p;
+            xi[++head] = w;
+            pushed = 1;
+            break;
+        }
+        if (!pushed) {
+            head--;
+            xi[--top] = v;
+        }
+    }
+    return top;
+}
+
+}  // namespace
+
+int pivot_factor(int n, const int* Ap, const int* Ai, const double* Ax,
+                 const int* q, double tol, PivotFactor& F) {
+    F.n = n;
+    F.singular_col = -1;
+    F.pinv.assign(n, -1);
+    F.Lp.assign(n + 1, 0);
+    F.Up.assign(n + 1, 0);
+    const long nnz = Ap[n];
+    long cap = 4 * nnz + n + 16;
+    F.Li.resize(cap);
+    F.Lx.resize(cap);
+    F.Ui.resize(cap);
+    F.Ux.resize(cap);
+    std::vector<int> xi(2 * (size_t)n + 1);
+    std::vector<unsigned char> mark(n, 0);
+    std::vector<double> x(n, 0.0);
+    int* pinv = F.pinv.data();
+    long lnz = 0, unz = 0;
+
+    for (int k = 0; k < n; k++) {
+        F.Lp[k] = (int)lnz;
+        F.Up[k] = (int)unz;
+        if ((long)F.Li.size() < lnz + n + 1) {
+            long nc = std::max<long>(2 * (long)F.Li.size(), lnz + n + 1);
+            F.Li.resize(nc);
+            F.Lx.resize(nc);
+        }
+        if ((long)F.Ui.size() < unz + n + 1) {
+            long nc = std::max<long>(2 * (long)F.Ui.size(), unz + n + 1);
+            F.Ui.resize(nc);
+            F.Ux.resize(nc);
+        }
+        const int col = q ? q[k] : k;
+        const int* Lp = F.Lp.data();
+        const int* Li = F.Li.data();
+        const double* Lx = F.Lx.data();
+
+        // Reach of A(:,col) in the graph of L (splu.h:109-123).
+        int top = n;
+        for (int p = Ap[col]; p < Ap[col + 1]; p++) {
+            if (!mark[Ai[p]])
+                top = dfs_from(Ai[p], Lp, Li, top, xi.data(), xi.data() + n, pinv, mark.data());
+        }
+        for (int p = top; p < n; p++) mark[xi[p]] = 0;
+
+        // Sparse triangular solve in topological order (splu.h:126-146).
+        for (int p = top; p < n; p++) x[xi[p]] = 0.0;
+        for (int p = Ap[col]; p < Ap[col + 1]; p++) x[Ai[p]] = Ax[p];
+        for (int px = top; px < n; px++) {
+            const int j = xi[px];
+            const int J = pinv[j];
+            if (J < 0) continue;
+            const double xj = x[j];   // L(J,J) == 1: the division is exact
+            for (int t = Lp[J] + 1; t < Lp[J + 1]; t++) x[Li[t]] -= Lx[t] * xj;
+        }
+
+        // Pivot: first strictly larger |x| in reach order; pivoted rows go
+        // to U (splu.h:174-187).
+        int ipiv = -1;
+        double amax = -1.0;
+        for (int p = top; p < n; p++) {
+            const int i = xi[p];
+            if (pinv[i] < 0) {
+                const double t = std::fabs(x[i]);
+                if (t > amax) { amax = t; ipiv = i; }
+            } else {
+                F.Ui[unz] = pinv[i];
+                F.Ux[unz++] = x[i];
+            }
+        }
+        if (ipiv == -1 || amax <= 0.0) {
+            F.singular_col = k;
+            F.Lp[n] = (int)lnz;
+            F.Up[n] = (int)unz;
+            return k;
+        }
+        if (pinv[col] < 0 && std::fabs(x[col]) >= amax * tol) ipiv = col;
+        const double pivot = x[ipiv];
+        F.Ui[unz] = k;
+        F.Ux[unz++] = pivot;
+        pinv[ipiv] = k;
+        F.Li[lnz] = ipiv;
+        F.Lx[lnz++] = 1.0;
+        for (int p = top; p < n; p++) {
+            const int i = xi[p];
+            if (pinv[i] < 0) {
+                F.Li[lnz] = i;
+                F.Lx[lnz++] = x[i] / pivot;
+            }
+            x[i] = 0.0;
+        }
+    }
+    F.Lp[n] = (int)lnz;
+    F.Up[n] = (int)unz;
+    for (long p = 0; p < lnz; p++) F.Li[p] = pinv[F.Li[p]];
+    F.Li.resize(lnz);
+    F.Lx.resize(lnz);
+    F.Ui.resize(unz);
+    F.Ux.resize(unz);
+    return -1;
+}
+
+uint64_t pattern_hash(int n, const int* Ap, const int* Ai, const int* q) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&h](uint32_t v) {
+        for (int b = 0; b < 4; b++) {
+            h ^= (v >> (8 * b)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    };
+    mix((uint32_t)n);
+    for (int i = 0; i <= n; i++) mix((uint32_t)Ap[i]);
+    for (int p = 0; p < Ap[n]; p++) mix((uint32_t)Ai[p]);
+    mix(q ? 1u : 0u);
+    if (q)
+        for (int i = 0; i < n; i++) mix((uint32_t)q[i]);
+    return h;
+}
+
+namespace {
+
+// Level of each item, given its dependency lists (deps all earlier in
+// `visit` order), then a stable counting sort by level.
+void levels_and_order(int n, const std::vector<int>& visit,
+                      const std::vector<int>& ptr, const std::vector<int>& dep,
+                      std::vector<int>& level, std::vector<int>& order,
+                      int& nlevels) {
+    level.assign(n, 0);
+    int maxl = -1;
+    for (int idx = 0; idx < n; idx++) {
+        const int i = visit[idx];
+        int l = 0;
+        for (int p = ptr[i]; p < ptr[i + 1]; p++) l = std::max(l, level[dep[p]] + 1);
+        level[i] = l;
+        maxl = std::max(maxl, l);
+    }
+    nlevels = maxl + 1;
+    std::vector<int> cnt(nlevels + 1, 0);
+    for (int i = 0; i < n; i++) cnt[level[i] + 1]++;
+    for (int l = 0; l < nlevels; l++) cnt[l + 1] += cnt[l];
+    order.assign(n, 0);
+    for (int idx = 0; idx < n; idx++) {
+        const int i = visit[idx];
+        order[cnt[level[i]]++] = i;
+    }
+}
+
+}  // namespace
+
+void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
+                          const PivotFactor& F, int sell_sigma, StaticPattern& S) {
+    S.n = n;
+    S.nnz_a = Ap[n];
+    S.lnnz = F.Lp[n];
+    S.unnz = F.Up[n];
+    S.cap = S.lnnz + S.unnz - n;
+    S.hash = pattern_hash(n, Ap, Ai, q);
+    S.q.resize(n);
+    S.invq.resize(n);
+    for (int k = 0; k < n; k++) S.q[k] = q ? q[k] : k;
+    for (int k = 0; k < n; k++) S.invq[S.q[k]] = k;
+    S.pinv = F.pinv;
+    S.rowat.assign(n, -1);
+    for (int i = 0; i < n; i++) S.rowat[S.pinv[i]] = i;
+
+    // Merged columns, rows ascending.
+    S.cp.assign(n + 1, 0);
+    S.dg.assign(n, 0);
+    S.ri.resize(S.cap);
+    S.max_col = 0;
+    {
+        long pos = 0;
+        std::vector<int> tmp;
+        for (int k = 0; k < n; k++) {
+            S.cp[k] = (int)pos;
+            tmp.clear();
+            for (int p = F.Up[k]; p < F.Up[k + 1] - 1; p++) tmp.push_back(F.Ui[p]);
+            std::sort(tmp.begin(), tmp.end());
+            for (int v : tmp) S.ri[pos++] = v;
+            S.dg[k] = (int)pos;
+            S.ri[pos++] = k;
+            tmp.clear();
+            for (int p = F.Lp[k] + 1; p < F.Lp[k + 1]; p++) tmp.push_back(F.Li[p]);
+            std::sort(tmp.begin(), tmp.end());
+            for (int v : tmp) S.ri[pos++] = v;
+            S.max_col = std::max(S.max_col, (int)(pos - S.cp[k]));
+        }
+        S.cp[n] = (int)pos;
+    }
+
+    // Refactorization schedule: column k depends on the rows j < k of U(:,k)
+    // (level.c:20-38 semantics), positions ascending are a topological order.
+    {
+        std::vector<int> ptr(n + 1), dep;
+        dep.reserve(S.unnz);
+        for (int k = 0; k < n; k++) {
+            ptr[k] = (int)dep.size();
+            for (int p = S.cp[k]; p < S.dg[k]; p++) dep.push_back(S.ri[p]);
+        }
+        ptr[n] = (int)dep.size();
+        std::vector<int> visit(n);
+        std::iota(visit.begin(), visit.end(), 0);
+        levels_and_order(n, visit, ptr, dep, S.col_level, S.col_order, S.ncol_levels);
+        long fl = 0, ga = 0;
+        for (int k = 0; k < n; k++)
+            for (int p = S.cp[k]; p < S.dg[k]; p++) {
+                const int j = S.ri[p];
+                const long lj = S.cp[j + 1] - S.dg[j] - 1;
+                fl += lj;
+                ga += lj;
+            }
+        S.flops = fl;
+        S.gathered = ga;
+    }
+
+    // Row-major copies of strict L and strict U.
+    {
+        S.lrp.assign(n + 1, 0);
+        S.urp.assign(n + 1, 0);
+        for (int k = 0; k < n; k++) {
+            for (int p = S.cp[k]; p < S.dg[k]; p++) S.urp[S.ri[p] + 1]++;
+            for (int p = S.dg[k] + 1; p < S.cp[k + 1]; p++) S.lrp[S.ri[p] + 1]++;
+        }
+        for (int i = 0; i < n; i++) {
+            S.lrp[i + 1] += S.lrp[i];
+            S.urp[i + 1] += S.urp[i];
+        }
+        S.lci.resize(S.lrp[n]);
+        S.uci.resize(S.urp[n]);
+        S.slot_dst.assign(S.cap, -1);
+        std::vector<int> lcur(S.lrp.begin(), S.lrp.end() - 1), ucur(S.urp.begin(), S.urp.end() - 1);
+        // Columns visited in ascending k: each row's entries come out with
+        // ascending column positions.
+        for (int k = 0; k < n; k++) {
+            for (int p = S.cp[k]; p < S.dg[k]; p++) {
+                const int i = S.ri[p];
+                const int d = ucur[i]++;
+                S.uci[d] = k;
+                S.slot_dst[p] = d;
+            }
+            S.slot_dst[S.dg[k]] = k;
+            for (int p = S.dg[k] + 1; p < S.cp[k + 1]; p++) {
+                const int i = S.ri[p];
+                const int d = lcur[i]++;
+                S.lci[d] = k;
+                S.slot_dst[p] = d;
+            }
+        }
+        // Forward levels: row i depends on columns of its L row (all < i).
+        std::vector<int> visit(n);
+        std::iota(visit.begin(), visit.end(), 0);
+        std::vector<int> lev;
+        levels_and_order(n, visit, S.lrp, S.lci, lev, S.fwd_order, S.nfwd_levels);
+        // Backward levels: row i depends on columns of its U row (all > i).
+        std::vector<int> rvisit(n);
+        for (int i = 0; i < n; i++) rvisit[i] = n - 1 - i;
+        levels_and_order(n, rvisit, S.urp, S.uci, lev, S.bwd_order, S.nbwd_levels);
+    }
+
+    // Input entries -> slots (column k = invq[c], row = pinv[orig row]).
+    {
+        S.a_ptr.assign(n + 1, 0);
+        for (int c = 0; c < n; c++) S.a_ptr[S.invq[c] + 1] += Ap[c + 1] - Ap[c];
+        for (int k = 0; k < n; k++) S.a_ptr[k + 1] += S.a_ptr[k];
+        S.a_src.resize(S.nnz_a);
+        S.a_dst.resize(S.nnz_a);
+        std::vector<std::pair<int, int>> tmp;
+        for (int k = 0; k < n; k++) {
+            const int c = S.q[k];
+            tmp.clear();
+            const int* rb = S.ri.data() + S.cp[k];
+            const int len = S.cp[k + 1] - S.cp[k];
+            for (int p = Ap[c]; p < Ap[c + 1]; p++) {
+                const int r = S.pinv[Ai[p]];
+                const int* it = std::lower_bound(rb, rb + len, r);
+                tmp.emplace_back((int)(it - rb), p);
+            }
+            std::stable_sort(tmp.begin(), tmp.end(),
+                             [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+                                 return a.first < b.first;
+                             });
+            int o = S.a_ptr[k];
+            for (auto& e : tmp) {
+                S.a_dst[o] = e.first;
+                S.a_src[o] = e.second;
+                o++;
+            }
+        }
+    }
+
+    // SELL-C-sigma (C = 32) copy of A in position space.
+    {
+        const int C = 32;
+        S.sell_sigma = std::max(C, sell_sigma);
+        // Row r (position) holds the input entries of original row rowat[r].
+        std::vector<int> rlen(n, 0);
+        for (int c = 0; c < n; c++)
+            for (int p = Ap[c]; p < Ap[c + 1]; p++) rlen[S.pinv[Ai[p]]]++;
+        std::vector<int> rptr(n + 1, 0);
+        for (int r = 0; r < n; r++) rptr[r + 1] = rptr[r] + rlen[r];
+        std::vector<int> rcol(S.nnz_a), rsrc(S.nnz_a);
+        {
+            std::vector<int> cur(rptr.begin(), rptr.end() - 1);
+            for (int k = 0; k < n; k++) {
+                const int c = S.q[k];
+                for (int p = Ap[c]; p < Ap[c + 1]; p++) {
+                    const int r = S.pinv[Ai[p]];
+                    const int d = cur[r]++;
+                    rcol[d] = k;
+                    rsrc[d] = p;
+                }
+            }
+        }
+        // Sort rows by descending length inside windows of sigma rows.
+        std::vector<int> perm(n);
+        std::iota(perm.begin(), perm.end(), 0);
+        for (int w0 = 0; w0 < n; w0 += S.sell_sigma) {
+            const int w1 = std::min(n, w0 + S.sell_sigma);
+            std::stable_sort(perm.begin() + w0, perm.begin() + w1,
+                             [&rlen](int a, int b) { return rlen[a] > rlen[b]; });
+        }
+        S.nslices = (n + C - 1) / C;
+        S.sell_ptr.assign(S.nslices + 1, 0);
+        S.sell_perm.assign((size_t)S.nslices * C, -1);
+        for (int s = 0; s < S.nslices; s++) {
+            int ml = 0;
+            for (int r = 0; r < C; r++) {
+                const int k = s * C + r;
+                if (k < n) {
+                    S.sell_perm[k] = perm[k];
+                    ml = std::max(ml, rlen[perm[k]]);
+                }
+            }
+            S.sell_ptr[s + 1] = S.sell_ptr[s] + ml * C;
+        }
+        const int total = S.sell_ptr[S.nslices];
+        S.sell_col.assign(total, 0);
+        S.sell_src.assign(total, -1);
+        for (int s = 0; s < S.nslices; s++) {
+            for (int r = 0; r < C; r++) {
+                const int k = s * C + r;
+                if (k >= n) continue;
+                const int row = perm[k];
+                for (int t = 0; t < rlen[row]; t++) {
+                    S.sell_col[S.sell_ptr[s] + t * C + r] = rcol[rptr[row] + t];
+                    S.sell_src[S.sell_ptr[s] + t * C + r] = rsrc[rptr[row] + t];
+                }
+                // Padding points at the row's own position: always a valid x.
+                for (int t = rlen[row]; t < (S.sell_ptr[s + 1] - S.sell_ptr[s]) / C; t++)
+                    S.sell_col[S.sell_ptr[s] + t * C + r] = row;
+            }
+        }
+    }
+}
+
+}  // namespace lusp

@@ -1,0 +1,129 @@
+"""Parity of the batched engine (refactor, solves) with the oracle, through
+the lusp_* C-ABI on the GPU."""
+import numpy as np
+import pytest
+
+from luspice_b200 import api, mna
+from tests.helpers import TOL_REL, oracle_refactor, oracle_solution, rel_err, rel_res, small_problems
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("prec", [api.MIXED, api.FP64])
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_refactor_bitwise(gpu, prec, idx):
+    """Frozen-pivot refactorization equals the host restatement bit for bit
+    (fp64 work vector, separately rounded multiply/subtract; fp32 storage on
+    the mixed path)."""
+    m = small_problems()[idx]
+    P = api.Pattern.from_matrix(m)
+    vals = m.perturbed(3, seed=100 + idx)
+    B = api.Batch([P] * 3, prec=prec)
+    B.upload(list(vals), [m.b] * 3)
+    B.run(api.RUN_REFACTOR)
+    st = B.stats()
+    for s in range(3):
+        got = B.factor_values(s)
+        exp, bad = oracle_refactor(m, P, vals[s], fp32=(prec == api.MIXED))
+        assert bad < 0
+        exp = exp.astype(got.dtype)
+        ity = np.uint32 if got.dtype == np.float32 else np.uint64
+        mism = np.flatnonzero(got.view(ity) != exp.view(ity))
+        assert mism.size == 0, f"system {s}: {mism.size} slots differ, first {mism[:5]}"
+        assert st[s]["status"] & api.ST_SINGULAR == 0
+
+
+@pytest.mark.parametrize("prec", [api.MIXED, api.FP64])
+def test_solve_matches_oracle(gpu, prec):
+    """Mixed (fp32 factors + fp64 GMRES-IR) and plain fp64 solves reach the
+    fp64 oracle solution within rel-L2 1e-6 for every perturbed system."""
+    m = mna.analog(989, 42)
+    P = api.Pattern.from_matrix(m)
+    vals = m.perturbed(4, seed=7)
+    B = api.Batch([P] * 4, prec=prec)
+    B.upload(list(vals), [m.b] * 4)
+    B.run(api.RUN_BOTH)
+    xs = B.split(B.download())
+    st = B.stats()
+    _, q = P.perm()
+    for s in range(4):
+        ref = oracle_solution(m, vals[s], q=q)
+        e = rel_err(xs[s], ref)
+        r = rel_res(m, vals[s], xs[s], m.b)
+        assert e <= TOL_REL, f"sys {s}: rel err {e:.3e} stats {st[s]}"
+        assert r <= 1e-9, f"sys {s}: residual {r:.3e} stats {st[s]}"
+        if prec == api.MIXED:
+            assert st[s]["status"] & api.ST_FAIL_MASK == 0, st[s]
+            assert st[s]["res"][-1] <= 1e-10
+
+
+def test_power_grid_batch(gpu):
+    m = mna.power_grid()
+    P = api.Pattern.from_matrix(m)
+    vals = m.perturbed(8, seed=11)
+    B = api.Batch([P] * 8, prec=api.MIXED)
+    B.upload(list(vals), [m.b] * 8)
+    B.run(api.RUN_BOTH)
+    xs = B.split(B.download())
+    _, q = P.perm()
+    for s in range(8):
+        ref = oracle_solution(m, vals[s], q=q)
+        assert rel_err(xs[s], ref) <= TOL_REL
+
+
+def test_uneven_batch_same_alone_and_mixed(gpu):
+    """Different patterns in one launch; each result equals the result of the
+    same system solved alone (bitwise: one CTA runs a system the same way)."""
+    ms = [mna.analog(int(n), 42 + i) for i, n in enumerate([150, 700, 333, 1200])]
+    pats = [api.Pattern.from_matrix(m) for m in ms]
+    B = api.Batch(pats, prec=api.MIXED)
+    B.upload([m.Ax for m in ms], [m.b for m in ms])
+    B.run(api.RUN_BOTH)
+    xs = B.split(B.download())
+    for i, m in enumerate(ms):
+        b1 = api.Batch([pats[i]], prec=api.MIXED)
+        b1.upload([m.Ax], [m.b])
+        b1.run(api.RUN_BOTH)
+        x1 = b1.download()
+        assert np.array_equal(x1, xs[i])
+        assert rel_err(xs[i], m.x_true) <= TOL_REL
+
+
+def test_graph_replay_matches(gpu):
+    m = mna.analog(500, 5)
+    P = api.Pattern.from_matrix(m)
+    vals = m.perturbed(2, seed=3)
+    B = api.Batch([P] * 2)
+    B.upload(list(vals), [m.b] * 2)
+    B.run(api.RUN_BOTH)
+    x0 = B.download()
+    B.run(api.RUN_BOTH, graph=True)
+    B.run(api.RUN_BOTH, graph=True)
+    x1 = B.download()
+    assert np.array_equal(x0, x1)
+
+
+def test_direct_solve_fp32_factors(gpu):
+    m = mna.analog(400, 9)
+    P = api.Pattern.from_matrix(m)
+    B = api.Batch([P])
+    B.upload([m.Ax], [m.b])
+    B.run(api.RUN_REFACTOR)
+    B.run(api.RUN_SOLVE | api.RUN_DIRECT)
+    x = B.download()
+    # fp32 factors alone: a few digits; the IR path restores the rest.
+    assert rel_err(x, m.x_true) < 1e-2
+    B.run(api.RUN_SOLVE)
+    assert rel_err(B.download(), m.x_true) <= TOL_REL
+
+
+def test_singular_flagged(gpu):
+    """A value set that zeroes a pivot is reported, not hidden."""
+    m = mna.analog(200, 13)
+    P = api.Pattern.from_matrix(m)
+    B = api.Batch([P], prec=api.FP64)
+    B.upload([np.zeros(m.nnz)], [m.b])
+    B.run(api.RUN_BOTH)
+    st = B.stats()[0]
+    assert st["status"] & api.ST_SINGULAR
+    assert st["singular_col"] >= 0
