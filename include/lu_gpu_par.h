@@ -80,6 +80,31 @@ int lusp_trisolve_par_launch(
     const int *Up, const int *Ui, const double *Ux,
     const int *pinv, const int *q, const double *b, double *x,
     int *work_i, double *work_d, void *stream);
+
+/* No counterpart in the reference.  The same solve as
+ * lusp_trisolve_par_launch for callers that cannot allocate device memory at
+ * solve time (a simulator time-step loop that sized all device memory up
+ * front and must not call cudaMalloc mid-run, which synchronizes the device
+ * and can fail with out-of-memory; host code that owns every device byte
+ * through its own arena): the work arrays come from a fixed scratch area
+ * inside the library instead of the caller.
+ *   - n <= LUSP_NOALLOC_MAX_N, else LUSP_EARG (3) and lusp_last_error() says
+ *     why; the scratch (1.25 MiB) is held by every GPU that loads the library
+ *     until the process exits.
+ *   - The first call on a device looks the scratch address up for that
+ *     device (make it with that device current); make this first call
+ *     before any stream capture.
+ *   - Allocates nothing: no cudaMalloc, no cudaFree.
+ *   - All calls share one scratch area per device: calls that overlap on the
+ *     GPU (different streams, or a second call before the first finished on
+ *     another stream) race and give wrong results; serialize them (one
+ *     stream, or events).  Nothing needs clearing between calls.
+ * Returns LUSP_OK (0), LUSP_EARG or LUSP_ECUDA (4). */
+#define LUSP_NOALLOC_MAX_N 65536
+int lusp_trisolve_par_noalloc(
+    int n, const int *Lp, const int *Li, const double *Lx,
+    const int *Up, const int *Ui, const double *Ux,
+    const int *pinv, const int *q, const double *b, double *x, void *stream);
 #ifdef __cplusplus
 }
 #endif

@@ -104,6 +104,7 @@ SIGNATURES = {
     "lusp_lu_factor_par_launch": (C.c_int, [C.c_int] + [C.c_void_p] * 7 + [C.c_long]
                                   + [C.c_void_p] * 3 + [C.c_long] + [C.c_void_p] * 7),
     "lusp_trisolve_par_launch": (C.c_int, [C.c_int] + [C.c_void_p] * 13),
+    "lusp_trisolve_par_noalloc": (C.c_int, [C.c_int] + [C.c_void_p] * 11),
     # lu_static.h
     "dsh_symbolic": (C.c_int, [C.c_int, C.c_long, c_int_p, c_int_p, c_int_p, C.POINTER(DshLuStatic)]),
     "dsh_numeric": (C.c_int, [C.POINTER(DshLuStatic), c_int_p, c_int_p, c_double_p, C.c_int]),
