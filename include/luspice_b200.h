@@ -78,6 +78,9 @@ typedef struct {
     double min_abs_pivot, min_pivot_ratio, max_abs_u;
     double res[16];                /* ||b - A x|| / ||b|| history */
     int nres, inner_iters, outer_iters, status, singular_col, pad_;
+    /* SM cycles summed over warps: refactor waits for dependency columns,
+     * gathers of their L parts, updates; refactor wall cycles of the CTA */
+    long long cyc_wait, cyc_gather, cyc_update, cyc_refactor;
 } lusp_sys_stats;
 
 typedef struct {
@@ -90,6 +93,12 @@ typedef struct {
     double pivot_tol;              /* frozen-pivot acceptance (default 1e-3) */
     int block_threads;             /* CTA size (default 256) */
     int ctas_per_sm;               /* shared-memory plan target (default 2) */
+    int solve_sweep;               /* triangular solves: 0 auto, 1 dataflow (per-row
+                                      ready bits), 2 level-synchronous (barrier per
+                                      level, descriptors in shared memory) */
+    int refactor_mode;             /* gathers of dependency columns: 0 staged in
+                                      shared memory by asynchronous copies, 1 loaded
+                                      per dependency */
 } lusp_batch_opts;
 
 /* ---- library ---- */

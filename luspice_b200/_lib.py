@@ -27,13 +27,15 @@ class SysStats(C.Structure):
     _fields_ = [("min_abs_pivot", C.c_double), ("min_pivot_ratio", C.c_double),
                 ("max_abs_u", C.c_double), ("res", C.c_double * 16), ("nres", C.c_int),
                 ("inner_iters", C.c_int), ("outer_iters", C.c_int), ("status", C.c_int),
-                ("singular_col", C.c_int), ("pad_", C.c_int)]
+                ("singular_col", C.c_int), ("pad_", C.c_int), ("cyc_wait", C.c_longlong),
+                ("cyc_gather", C.c_longlong), ("cyc_update", C.c_longlong), ("cyc_refactor", C.c_longlong)]
 
 
 class BatchOpts(C.Structure):
     _fields_ = [("prec", C.c_int), ("krylov", C.c_int), ("max_outer", C.c_int),
                 ("rtol", C.c_double), ("inner_rel", C.c_double), ("stag_ratio", C.c_double),
-                ("pivot_tol", C.c_double), ("block_threads", C.c_int), ("ctas_per_sm", C.c_int)]
+                ("pivot_tol", C.c_double), ("block_threads", C.c_int), ("ctas_per_sm", C.c_int),
+                ("solve_sweep", C.c_int), ("refactor_mode", C.c_int)]
 
 
 class DshLuStatic(C.Structure):

@@ -148,6 +148,8 @@ void lusp_batch_opts_default(lusp_batch_opts* o) {
     o->pivot_tol = 1e-3;
     o->block_threads = 256;
     o->ctas_per_sm = 2;
+    o->solve_sweep = 0;
+    o->refactor_mode = 0;
 }
 
 int lusp_batch_create(int nsys, lusp_pattern* const* pats, const lusp_batch_opts* opts,

@@ -134,7 +134,7 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     const std::vector<int>* arrays[] = {&S.cp, &S.ri, &S.dg, &S.col_order, &S.a_ptr, &S.a_src, &S.a_dst,
                                         &S.lrp, &S.lci, &S.urp, &S.uci, &S.slot_dst, &S.fwd_order,
                                         &S.bwd_order, &S.sell_ptr, &S.sell_col, &S.sell_src,
-                                        &S.sell_perm, &S.rowat, &S.q};
+                                        &S.sell_perm, &S.rowat, &S.q, &S.fwd_lev, &S.bwd_lev};
     const int narr = (int)(sizeof(arrays) / sizeof(arrays[0]));
     std::vector<size_t> off(narr + 1, 0);
     for (int a = 0; a < narr; a++) off[a + 1] = off[a] + ((arrays[a]->size() + 31) & ~(size_t)31);
@@ -177,6 +177,10 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     D.sell_perm = blk + off[idx++];
     D.rowat = blk + off[idx++];
     D.q = blk + off[idx++];
+    D.fwd_lev = blk + off[idx++];
+    D.bwd_lev = blk + off[idx++];
+    D.nfwd_levels = S.nfwd_levels;
+    D.nbwd_levels = S.nbwd_levels;
     e = cudaMalloc(&P->d_desc, sizeof(PatternDev));
     if (e != cudaSuccess) { pattern_free(P); return cuda_fail(e, "pattern descriptor alloc"); }
     e = cudaMemcpy(P->d_desc, &D, sizeof(PatternDev), cudaMemcpyHostToDevice);
@@ -209,11 +213,13 @@ static int sm_count() {
 
 static size_t smem_fixed(int nwords) { return 64 + (((size_t)nwords * 4 + 15) & ~(size_t)15) + 40 * sizeof(double); }
 
-void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm, int m, SmemPlan& plan) {
-    int nmax = 1, colmax = 1;
+void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm, int m, int vsize,
+               SmemPlan& plan) {
+    int nmax = 1, colmax = 1, levmax = 1;
     for (auto* p : pats) {
         nmax = std::max(nmax, p->S.n);
         colmax = std::max(colmax, p->S.max_col);
+        levmax = std::max(levmax, p->S.nfwd_levels + p->S.nbwd_levels);
     }
     const size_t limit = 227 * 1024;
     size_t budget = 228 * 1024 / std::max(1, ctas_per_sm);
@@ -225,14 +231,30 @@ void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm,
     const int nw = block / 32;
     const size_t hbytes = ((size_t)(m + 1) * m + 6 * (size_t)(m + 1)) * sizeof(double);
     size_t avail = budget > fixed + hbytes ? budget - fixed - hbytes : 0;
-    // Solve vector in shared memory when it fits.
+    // Solve vector in shared memory when it fits, and the level-sweep
+    // descriptors (row order, row pointers, level bounds of both sweeps)
+    // when they fit beside it.
     plan.ycap = ((size_t)nmax * 8 <= avail) ? nmax : 0;
-    // Refactor work area per warp.
-    size_t ravail = budget > fixed ? budget - fixed : 0;
-    int wcap = (int)std::min<size_t>((size_t)colmax, ravail / ((size_t)nw * 12));
-    plan.wcap = std::max(wcap, 0);
-    const size_t solve_bytes = (size_t)plan.ycap * 8 + hbytes;
-    const size_t ref_bytes = (size_t)plan.wcap * nw * 12;
+    const size_t dneed = 4 * (size_t)nmax + (size_t)levmax + 8;
+    plan.dcap = (plan.ycap && (size_t)nmax * 8 + dneed * 4 <= avail) ? (int)dneed : 0;
+    // Refactor area per warp: the work vector and rows of one column (up to
+    // the longest column; longer ones spill to global scratch) plus a stage
+    // of 512 gathered L entries (at least 64).
+    const size_t per_warp = budget > fixed ? (budget - fixed) / nw : 0;
+    const size_t stage_entry = 4 + (size_t)vsize;
+    int scap = 512;
+    while (scap > 64 && (size_t)scap * stage_entry > per_warp / 2) scap /= 2;
+    size_t left = per_warp > (size_t)scap * stage_entry ? per_warp - (size_t)scap * stage_entry : 0;
+    plan.wcap = (int)std::min<size_t>((size_t)colmax, left / 12);
+    plan.scap = scap;
+    // Row -> slot map (16-bit slots, n entries per warp) when it fits in what
+    // is left: replaces a binary search per gathered entry by one lookup.
+    left = left > (size_t)plan.wcap * 12 ? left - (size_t)plan.wcap * 12 : 0;
+    const size_t mneed = (((size_t)nmax * 2 + 15) & ~(size_t)15) / 2;
+    plan.mcap = (nmax <= 65535 && colmax <= 65535 && mneed * 2 <= left) ? (int)mneed : 0;
+    const size_t solve_bytes = (size_t)plan.ycap * 8 + hbytes + (size_t)plan.dcap * 4;
+    const size_t ref_bytes = (size_t)nw * ((size_t)plan.wcap * 12 + (size_t)plan.scap * stage_entry +
+                                           (size_t)plan.mcap * 2);
     plan.bytes = fixed + std::max(solve_bytes, ref_bytes);
 }
 
@@ -287,7 +309,14 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     B->prm.inner_rel = o->inner_rel;
     B->prm.stag_ratio = o->stag_ratio;
     B->prm.pivot_tol = o->pivot_tol;
-    make_plan(B->pats, B->block, o->ctas_per_sm, o->krylov, B->plan);
+    B->prm.refactor_mode = o->refactor_mode;
+    make_plan(B->pats, B->block, o->ctas_per_sm, o->krylov, B->prec == LUSP_FP64 ? 8 : 4, B->plan);
+    if (o->solve_sweep == 1) B->plan.dcap = 0;   // dataflow sweeps only
+    if (o->solve_sweep == 2 && B->plan.dcap == 0) {
+        set_error("batch_create: level-synchronous sweeps need the solve vector and descriptors in shared memory");
+        delete B;
+        return LUSP_EARG;
+    }
 
     const size_t vs = B->prec == LUSP_FP64 ? 8 : 4;
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };

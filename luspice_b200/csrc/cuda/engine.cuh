@@ -18,6 +18,7 @@ namespace lusp {
 struct PatternDev {
     int n, nnz_a, cap, max_col, nslices, sell_total;
     int nnz_l, nnz_u;        // strict L and strict U entries
+    int nfwd_levels, nbwd_levels;
     const int* cp;           // [n+1] merged column pointers
     const int* ri;           // [cap] row positions, ascending per column
     const int* dg;           // [n]   slot of the diagonal
@@ -25,13 +26,15 @@ struct PatternDev {
     const int* a_ptr;        // [n+1] input entries per column
     const int* a_src;        // [nnz_a] input index
     const int* a_dst;        // [nnz_a] slot offset inside the column
-    const int* lrp;          // [n+1] strict-L rows
+    const int* lrp;          // [n+1] strict-L rows in level order (by idx)
     const int* lci;          // [nnz_l] column positions
-    const int* urp;          // [n+1] strict-U rows
+    const int* urp;          // [n+1] strict-U rows in level order (by idx)
     const int* uci;          // [nnz_u] column positions
-    const int* slot_dst;     // [cap] slot -> L-CSR / U-CSR index, diag -> k
-    const int* fwd_order;    // [n] level-sorted rows for L y = b
-    const int* bwd_order;    // [n] level-sorted rows for U z = y
+    const int* slot_dst;     // [cap] slot -> L-row / U-row index, diag -> k
+    const int* fwd_order;    // [n] idx -> row, level-sorted, for L y = b
+    const int* bwd_order;    // [n] idx -> row, level-sorted, for U z = y
+    const int* fwd_lev;      // [nfwd_levels+1] first idx of each level
+    const int* bwd_lev;      // [nbwd_levels+1]
     const int* sell_ptr;     // [nslices+1]
     const int* sell_col;     // [sell_total] column positions
     const int* sell_src;     // [sell_total] input index or -1
@@ -52,6 +55,9 @@ struct SysStats {
     int status;
     int singular_col;
     int pad_;
+    // SM cycles (summed over warps): refactor waits for dependency columns,
+    // gathers of their L parts, updates; refactor wall cycles of the CTA.
+    long long cyc_wait, cyc_gather, cyc_update, cyc_refactor;
 };
 
 // One system: pattern + values + vectors + workspace.
@@ -79,6 +85,7 @@ struct SolveParams {
     double inner_rel;        // inner stop relative to the current residual
     double stag_ratio;       // residual must shrink by this factor per outer
     double pivot_tol;        // frozen-pivot acceptance threshold
+    int refactor_mode;       // 0 staged gathers (cp.async), 1 per-dependency loads
 };
 
 constexpr int kMaxKrylov = 64;
@@ -87,7 +94,10 @@ constexpr int kMaxKrylov = 64;
 struct SmemPlan {
     int nwords;              // ready-bit words (>= ceil(n_max/32))
     int wcap;                // per-warp refactor work slots
+    int scap;                // per-warp staged L entries (refactor gathers)
+    int mcap;                // per-warp row -> slot map entries (0 = none)
     int ycap;                // doubles for a shared-memory solve vector
+    int dcap;                // ints for shared-memory sweep descriptors
     int m;                   // Krylov dimension for H
     size_t bytes;
 };

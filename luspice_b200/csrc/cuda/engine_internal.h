@@ -56,7 +56,7 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
                   PatternObj** out);
 void pattern_free(PatternObj* P);
 
-void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm, int m,
+void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm, int m, int vsize,
                SmemPlan& plan);
 int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, BatchObj** out);
 void batch_free(BatchObj* B);

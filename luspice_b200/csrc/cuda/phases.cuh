@@ -26,6 +26,41 @@ struct Smem {
 // Status bits that describe a solve (cleared when a new solve starts).
 constexpr int kSolveBits = ST_STAGNATED | ST_NOT_CONVERGED | ST_NONFINITE | ST_WAIT_TIMEOUT;
 
+// Slot of row i among rows[lo, hi) (ascending), or -1.
+__device__ __forceinline__ int find_slot(const int* rows, int lo, int hi, int i) {
+    const int end = hi;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (rows[mid] < i) lo = mid + 1; else hi = mid;
+    }
+    return (lo < end && rows[lo] == i) ? lo : -1;
+}
+
+// Slot of row i through the column's row -> slot map, or -1.
+__device__ __forceinline__ int map_slot(const unsigned short* map, const int* rows, int len, int i) {
+    const int s = map[i];
+    return (s < len && rows[s] == i) ? s : -1;
+}
+
+// Non-blocking test of a ready bit.
+__device__ __forceinline__ bool is_ready(const unsigned* bits, int j) {
+    return (*((const volatile unsigned*)bits + (j >> 5)) >> (j & 31)) & 1u;
+}
+
+// Asynchronous global->shared copies (sm_80+ cp.async, L1-allocating):
+// issued without waiting, completed by cp_async_wait_all().
+__device__ __forceinline__ void cp_async_4(void* sdst, const void* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_8(void* sdst, const void* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_val(float* sdst, const float* gsrc) { cp_async_4(sdst, gsrc); }
+__device__ __forceinline__ void cp_async_val(double* sdst, const double* gsrc) { cp_async_8(sdst, gsrc); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __device__ __forceinline__ int warp_claim(int* counter) {
     int idx = 0;
     if ((threadIdx.x & 31) == 0) idx = atomicAdd(counter, 1);
@@ -52,8 +87,18 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
     const int n = P.n;
     Smem sm(smem_base, plan);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    // Per warp: work vector x[wcap] (fp64), staged values sval[scap] (VT),
+    // column rows wr[wcap], staged rows srow[scap].
     double* wx = (double*)sm.uni + (size_t)warp * plan.wcap;
-    int* wr = (int*)((double*)sm.uni + (size_t)nw * plan.wcap) + (size_t)warp * plan.wcap;
+    VT* sval_all = (VT*)((double*)sm.uni + (size_t)nw * plan.wcap);
+    VT* sval = sval_all + (size_t)warp * plan.scap;
+    int* wr = (int*)(sval_all + (size_t)nw * plan.scap) + (size_t)warp * plan.wcap;
+    int* srow = (int*)(sval_all + (size_t)nw * plan.scap) + (size_t)nw * plan.wcap + (size_t)warp * plan.scap;
+    // Optional per-warp row -> slot map (n entries, 16 bit).
+    unsigned short* wmap = (unsigned short*)((int*)(sval_all + (size_t)nw * plan.scap) +
+                                             (size_t)nw * (plan.wcap + plan.scap)) +
+                           (size_t)warp * plan.mcap;
+    const bool use_map = plan.mcap >= n;
 
     for (int t = threadIdx.x; t < (n + 31) / 32; t += blockDim.x) sm.ready[t] = 0u;
     if (threadIdx.x == 0) {
@@ -77,6 +122,14 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
     VT* udiag = (VT*)S.udiag;
     double minpiv = INFINITY, minratio = INFINITY, maxu = 0.0;
     int bad = 0;
+    long long c_wait = 0, c_gather = 0, c_update = 0;
+    const long long t_begin = clock64();
+    if (threadIdx.x == 0) {
+        S.stats->cyc_wait = 0;
+        S.stats->cyc_gather = 0;
+        S.stats->cyc_update = 0;
+    }
+    __syncthreads();
 
     while (true) {
         const int idx = warp_claim(&sm.ctl[0]);
@@ -111,30 +164,111 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 x[dst] = s;
             }
         }
+        // Row -> slot map of this column (when the plan has room for one):
+        // entries of other rows are stale, but only rows of this column's
+        // pattern are looked up (the static pattern is closed under the
+        // updates), and map_slot verifies the hit.
+        const bool cmap = use_map && rows == wr;
+        if (cmap)
+            for (int t = lane; t < len; t += 32) wmap[rows[t]] = (unsigned short)t;
         __syncwarp();
-        for (int u = 0; u < d; u++) {
-            const int j = rows[u];
-            if (!wait_ready(sm.ready, j, &sm.ctl[3])) bad |= ST_WAIT_TIMEOUT;
-            __syncwarp();
+        long long tc = clock64();
+        // Apply the dependency columns in ascending order.  Each round takes
+        // the next run of dependencies that are already complete (blocking
+        // only when the very next one is not, so the older dependencies of a
+        // column overlap with the computation of its most recent ones), up to
+        // plan.scap gathered entries; their L parts are copied to shared
+        // memory with all copies in flight together, then applied.
+        for (int u0 = 0; u0 < d;) {
+            const int u = u0 + lane;
+            int beg = 0, cnt = 0;
+            bool rdy = true;
+            if (u < d) {
+                const int jj = rows[u];
+                beg = P.dg[jj] + 1;
+                cnt = P.cp[jj + 1] - beg;
+                rdy = is_ready(sm.ready, jj);
+            }
+            int nready = __ffs(~__ballot_sync(0xffffffffu, rdy)) - 1;
+            if (nready < 0) nready = 32;
+            if (nready == 0) {
+                if (!wait_ready(sm.ready, rows[u0], &sm.ctl[3])) bad |= ST_WAIT_TIMEOUT;
+                __syncwarp();
+                nready = 1;
+            }
             __threadfence_block();
-            const double xj = x[u];
-            if (xj != 0.0) {
-                const int p0 = P.dg[j] + 1, p1 = P.cp[j + 1];
-                for (int p = p0 + lane; p < p1; p += 32) {
-                    const int i = P.ri[p];
-                    const double l = ValTraits<VT>::load(lu + p);
-                    int lo = u + 1, hi = len;
-                    while (lo < hi) {
-                        const int mid = (lo + hi) >> 1;
-                        if (rows[mid] < i) lo = mid + 1; else hi = mid;
+            {
+                const long long t2 = clock64();
+                c_wait += t2 - tc;
+                tc = t2;
+            }
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int excl = incl - cnt;
+            int nfit = prm.refactor_mode == 1
+                           ? 0
+                           : __popc(__ballot_sync(0xffffffffu, u < d && incl <= plan.scap));
+            nfit = min(nfit, nready);
+            if (nfit == 0) {
+                // One dependency longer than the stage: apply it from global.
+                const double xj = x[u0];
+                const int p0 = __shfl_sync(0xffffffffu, beg, 0);
+                const int p1 = p0 + __shfl_sync(0xffffffffu, cnt, 0);
+                if (xj != 0.0) {
+                    for (int p = p0 + lane; p < p1; p += 32) {
+                        const int i = P.ri[p];
+                        const double l = ValTraits<VT>::load(lu + p);
+                        const int s = cmap ? map_slot(wmap, rows, len, i) : find_slot(rows, u0 + 1, len, i);
+                        if (s >= 0) x[s] = __dsub_rn(x[s], __dmul_rn(l, xj));
+                        else bad |= ST_CAPACITY;
                     }
-                    if (lo < len && rows[lo] == i)
-                        x[lo] = __dsub_rn(x[lo], __dmul_rn(l, xj));
-                    else
-                        bad |= ST_CAPACITY;
+                }
+                __syncwarp();
+                u0 += 1;
+                continue;
+            }
+            for (int t = 0; t < nfit; t++) {
+                const int b_t = __shfl_sync(0xffffffffu, beg, t);
+                const int c_t = __shfl_sync(0xffffffffu, cnt, t);
+                const int o_t = __shfl_sync(0xffffffffu, excl, t);
+                for (int e = lane; e < c_t; e += 32) {
+                    cp_async_4(srow + o_t + e, P.ri + b_t + e);
+                    cp_async_val(sval + o_t + e, lu + b_t + e);
                 }
             }
+            cp_async_wait_all();
             __syncwarp();
+            {
+                const long long t2 = clock64();
+                c_gather += t2 - tc;
+                tc = t2;
+            }
+            for (int t = 0; t < nfit; t++) {
+                const int c_t = __shfl_sync(0xffffffffu, cnt, t);
+                const int o_t = __shfl_sync(0xffffffffu, excl, t);
+                const int uu = u0 + t;
+                const double xj = x[uu];
+                if (xj != 0.0) {
+                    for (int e = lane; e < c_t; e += 32) {
+                        const int i = srow[o_t + e];
+                        const double l = ValTraits<VT>::load(sval + o_t + e);
+                        const int s = cmap ? map_slot(wmap, rows, len, i) : find_slot(rows, uu + 1, len, i);
+                        if (s >= 0) x[s] = __dsub_rn(x[s], __dmul_rn(l, xj));
+                        else bad |= ST_CAPACITY;
+                    }
+                }
+                __syncwarp();
+            }
+            {
+                const long long t2 = clock64();
+                c_update += t2 - tc;
+                tc = t2;
+            }
+            u0 += nfit;
         }
         const double piv = x[d];
         double amax = 0.0;
@@ -166,6 +300,12 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         if (lane == 0) set_ready(sm.ready, k);
     }
 
+    if (lane == 0) {
+        atomicAdd((unsigned long long*)&S.stats->cyc_wait, (unsigned long long)c_wait);
+        atomicAdd((unsigned long long*)&S.stats->cyc_gather, (unsigned long long)c_gather);
+        atomicAdd((unsigned long long*)&S.stats->cyc_update, (unsigned long long)c_update);
+    }
+    if (threadIdx.x == 0) S.stats->cyc_refactor = clock64() - t_begin;
     // Statistics: warp reductions, then per-warp partials combined in order.
     minpiv = warp_min(minpiv);
     minratio = warp_min(minratio);
@@ -229,7 +369,7 @@ __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval
         const int idx = warp_claim(&sm.ctl[0]);
         if (idx >= n) break;
         const int i = P.fwd_order[idx];
-        const int p0 = P.lrp[i], p1 = P.lrp[i + 1];
+        const int p0 = P.lrp[idx], p1 = P.lrp[idx + 1];
         double acc = 0.0;
         for (int p = p0 + lane; p < p1; p += 32) {
             const int j = P.lci[p];
@@ -253,7 +393,7 @@ __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval
         const int idx = warp_claim(&sm.ctl[0]);
         if (idx >= n) break;
         const int i = P.bwd_order[idx];
-        const int p0 = P.urp[i], p1 = P.urp[i + 1];
+        const int p0 = P.urp[idx], p1 = P.urp[idx + 1];
         double acc = 0.0;
         for (int p = p0 + lane; p < p1; p += 32) {
             const int j = P.uci[p];
@@ -270,6 +410,131 @@ __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval
         }
     }
     __syncthreads();
+}
+
+// One triangular sweep, level-synchronous: the rows of a level are spread
+// over the warps (one warp per row, lanes over the row's entries), one
+// barrier per level.  Row order, row pointers and level bounds come from
+// shared memory; each warp keeps the first 32 entries (one per lane) of its
+// next two rows in registers (sets A and B, used alternately so a pending
+// load is never copied), loaded while earlier rows and barriers complete.
+// UPPER: y[i] = (y[i] - sum) / diag[i] (U sweep), else y[i] -= sum.
+template <typename VT, bool UPPER>
+__device__ void level_sweep(int nlev, const int* lev, const int* order, const int* rp,
+                            const int* ci, const VT* val, const VT* diag, double* y) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int gl = 0, gidx = warp;
+    while (gl < nlev && gidx >= lev[gl + 1]) {
+        gl++;
+        if (gl < nlev) gidx = lev[gl] + warp;
+    }
+    int a_idx = -1, a_lvl = nlev, a_col = -1, b_idx = -1, b_lvl = nlev, b_col = -1;
+    double a_v = 0.0, a_d = 1.0, b_v = 0.0, b_d = 1.0;
+#define LUSP_FETCH(IDX, LVL, COL, V, D)                                            \
+    if (gl < nlev) {                                                              \
+        IDX = gidx;                                                               \
+        LVL = gl;                                                                 \
+        const int pp = rp[gidx] + lane;                                           \
+        COL = -1;                                                                 \
+        V = 0.0;                                                                  \
+        if (pp < rp[gidx + 1]) {                                                  \
+            COL = ci[pp];                                                         \
+            V = ValTraits<VT>::load(val + pp);                                    \
+        }                                                                         \
+        if (UPPER) D = ValTraits<VT>::load(diag + order[gidx]);                   \
+        gidx += nw;                                                               \
+        while (gl < nlev && gidx >= lev[gl + 1]) {                                \
+            gl++;                                                                 \
+            if (gl < nlev) gidx = lev[gl] + warp;                                 \
+        }                                                                         \
+    } else {                                                                      \
+        IDX = -1;                                                                 \
+        LVL = nlev;                                                               \
+    }
+#define LUSP_ROW(IDX, COL, V, D)                                                   \
+    {                                                                             \
+        const int i = order[IDX];                                                 \
+        const int p1 = rp[IDX + 1];                                               \
+        double acc = COL >= 0 ? V * y[COL] : 0.0;                                 \
+        for (int p = rp[IDX] + 32 + lane; p < p1; p += 32)                        \
+            acc = fma(ValTraits<VT>::load(val + p), y[ci[p]], acc);               \
+        acc = warp_sum(acc);                                                      \
+        if (lane == 0) y[i] = UPPER ? (y[i] - acc) / D : y[i] - acc;              \
+    }
+    LUSP_FETCH(a_idx, a_lvl, a_col, a_v, a_d)
+    LUSP_FETCH(b_idx, b_lvl, b_col, b_v, b_d)
+    int passed = 0;   // barriers passed = levels known complete
+    while (true) {
+        if (a_idx < 0) break;
+        while (passed < a_lvl) { __syncthreads(); passed++; }
+        LUSP_ROW(a_idx, a_col, a_v, a_d)
+        LUSP_FETCH(a_idx, a_lvl, a_col, a_v, a_d)
+        if (b_idx < 0) break;
+        while (passed < b_lvl) { __syncthreads(); passed++; }
+        LUSP_ROW(b_idx, b_col, b_v, b_d)
+        LUSP_FETCH(b_idx, b_lvl, b_col, b_v, b_d)
+    }
+    while (passed < nlev) { __syncthreads(); passed++; }
+#undef LUSP_FETCH
+#undef LUSP_ROW
+}
+
+// Shared-memory sweep descriptors of one system: [fwd_order n][fwd rp n+1]
+// [fwd_lev nfl+1][bwd_order n][bwd rp n+1][bwd_lev nbl+1].
+__device__ __forceinline__ bool sweep_desc_fits(const PatternDev& P, const SmemPlan& plan) {
+    return P.n <= plan.ycap && 4 * P.n + P.nfwd_levels + P.nbwd_levels + 4 <= plan.dcap;
+}
+
+__device__ __forceinline__ int* sweep_desc_base(const SmemPlan& plan, Smem& sm) {
+    return (int*)((double*)sm.uni + plan.ycap + (size_t)(plan.m + 1) * plan.m + 6 * (size_t)(plan.m + 1));
+}
+
+__device__ void load_sweep_desc(const PatternDev& P, int* d) {
+    const int n = P.n, nfl = P.nfwd_levels, nbl = P.nbwd_levels;
+    int* f_ord = d;
+    int* f_rp = f_ord + n;
+    int* f_lev = f_rp + n + 1;
+    int* b_ord = f_lev + nfl + 1;
+    int* b_rp = b_ord + n;
+    int* b_lev = b_rp + n + 1;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        f_ord[t] = P.fwd_order[t];
+        b_ord[t] = P.bwd_order[t];
+    }
+    for (int t = threadIdx.x; t <= n; t += blockDim.x) {
+        f_rp[t] = P.lrp[t];
+        b_rp[t] = P.urp[t];
+    }
+    for (int t = threadIdx.x; t <= nfl; t += blockDim.x) f_lev[t] = P.fwd_lev[t];
+    for (int t = threadIdx.x; t <= nbl; t += blockDim.x) b_lev[t] = P.bwd_lev[t];
+}
+
+// y := U^-1 L^-1 rhs with the level-synchronous sweeps (descriptors already
+// in shared memory at d).
+template <typename VT>
+__device__ void cta_lu_apply_levels(const PatternDev& P, const VT* lval, const VT* uval,
+                                    const VT* udiag, const double* rhs, double* y, const int* d) {
+    const int n = P.n, nfl = P.nfwd_levels, nbl = P.nbwd_levels;
+    const int* f_ord = d;
+    const int* f_rp = f_ord + n;
+    const int* f_lev = f_rp + n + 1;
+    const int* b_ord = f_lev + nfl + 1;
+    const int* b_rp = b_ord + n;
+    const int* b_lev = b_rp + n + 1;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = rhs[i];
+    __syncthreads();
+    level_sweep<VT, false>(nfl, f_lev, f_ord, f_rp, P.lci, lval, udiag, y);
+    level_sweep<VT, true>(nbl, b_lev, b_ord, b_rp, P.uci, uval, udiag, y);
+}
+
+// Dispatch: level-synchronous sweeps when their descriptors sit in shared
+// memory (desc != nullptr), else the dataflow version.
+template <typename VT>
+__device__ __forceinline__ void lu_apply(const PatternDev& P, const VT* lval, const VT* uval,
+                                         const VT* udiag, const double* rhs, double* y,
+                                         Smem& sm, const int* desc, int& bad) {
+    if (desc) cta_lu_apply_levels<VT>(P, lval, uval, udiag, rhs, y, desc);
+    else cta_lu_apply<VT>(P, lval, uval, udiag, rhs, y, sm, bad);
 }
 
 // out = A x (RESID: out = bt - A x) with A in SELL-C-sigma, C = 32, values AT.
@@ -312,8 +577,14 @@ __device__ void direct_phase(const SysDev& S, const SmemPlan& plan, char* smem_b
     if (threadIdx.x == 0) S.stats->status &= ~kSolveBits;
     for (int i = threadIdx.x; i < n; i += blockDim.x) bt[i] = S.b[P.rowat[i]];
     __syncthreads();
+    const int* desc = nullptr;
+    if (sweep_desc_fits(P, plan)) {
+        int* d = sweep_desc_base(plan, sm);
+        load_sweep_desc(P, d);
+        desc = d;
+    }
     const double nb = sqrt(cta_dot(bt, bt, n, sm));
-    cta_lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, bt, y, sm, bad);
+    lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, bt, y, sm, desc, bad);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         xt[i] = y[i];
         S.x[P.q[i]] = y[i];
@@ -379,6 +650,12 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         bt[i] = S.b[P.rowat[i]];
         xt[i] = 0.0;
     }
+    const int* desc = nullptr;
+    if (sweep_desc_fits(P, plan)) {
+        int* d = sweep_desc_base(plan, sm);
+        load_sweep_desc(P, d);
+        desc = d;
+    }
     __syncthreads();
     const double nb = sqrt(cta_dot(bt, bt, n, sm));
     if (!(nb > 0.0)) {
@@ -420,7 +697,7 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         int jj = 0;
         for (int j = 0; j < m; j++) {
             const double* vj = V + (size_t)j * n;
-            cta_lu_apply<VT>(P, lval, uval, udiag, vj, y, sm, bad);
+            lu_apply<VT>(P, lval, uval, udiag, vj, y, sm, desc, bad);
             cta_spmv<AT, false>(P, ainner, y, nullptr, w);
             __syncthreads();
             const double wn0 = sqrt(cta_dot(w, w, n, sm));
@@ -489,7 +766,7 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
             z[e] = acc;
         }
         __syncthreads();
-        cta_lu_apply<VT>(P, lval, uval, udiag, z, y, sm, bad);
+        lu_apply<VT>(P, lval, uval, udiag, z, y, sm, desc, bad);
         for (int e = threadIdx.x; e < n; e += blockDim.x) xt[e] += y[e];
         __syncthreads();
         outer_done++;

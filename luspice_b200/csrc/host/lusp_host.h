@@ -52,18 +52,19 @@ struct StaticPattern {
     // inside column k), sorted by a_dst (duplicates adjacent).
     std::vector<int> a_ptr, a_src, a_dst;
 
-    // Row-major copies for the triangular solves.
-    // L (strictly lower, unit diagonal implicit): rows by position.
-    std::vector<int> lrp, lci;      // lci: column positions, ascending
-    // U (strictly upper): rows by position, column positions ascending.
+    // Row-major copies for the triangular solves, rows stored in level
+    // order: strict-L row fwd_order[idx] is [lrp[idx], lrp[idx+1]) of lci
+    // (column positions ascending); strict-U row bwd_order[idx] likewise in
+    // urp/uci.  fwd_lev / bwd_lev: first idx of each level (+ end).
+    std::vector<int> lrp, lci;
     std::vector<int> urp, uci;
-    // slot -> destination: L slots -> index in L-CSR, U slots -> index in
-    // U-CSR, diagonal slot -> k.
+    // slot -> destination: L slots -> index in the L rows, U slots -> index
+    // in the U rows, diagonal slot -> k.
     std::vector<int> slot_dst;
     std::vector<int> fwd_order, bwd_order;   // level-sorted row orders
+    std::vector<int> fwd_lev, bwd_lev;
     int nfwd_levels = 0, nbwd_levels = 0;
 
-    // Depth-first critical path lengths (longest chain of dependencies).
     // SELL-C-sigma copy of A in position space (C = 32): slice s covers
     // sorted rows [32 s, 32 s + 32); entry (r, t) of slice s is at
     // sell_ptr[s] + 32 t + r.  sell_perm[32 s + r] = row position (-1 pad),

@@ -179,7 +179,7 @@ namespace {
 void levels_and_order(int n, const std::vector<int>& visit,
                       const std::vector<int>& ptr, const std::vector<int>& dep,
                       std::vector<int>& level, std::vector<int>& order,
-                      int& nlevels) {
+                      int& nlevels, std::vector<int>* level_ptr = nullptr) {
     level.assign(n, 0);
     int maxl = -1;
     for (int idx = 0; idx < n; idx++) {
@@ -193,6 +193,7 @@ void levels_and_order(int n, const std::vector<int>& visit,
     std::vector<int> cnt(nlevels + 1, 0);
     for (int i = 0; i < n; i++) cnt[level[i] + 1]++;
     for (int l = 0; l < nlevels; l++) cnt[l + 1] += cnt[l];
+    if (level_ptr) level_ptr->assign(cnt.begin(), cnt.end());
     order.assign(n, 0);
     for (int idx = 0; idx < n; idx++) {
         const int i = visit[idx];
@@ -305,11 +306,37 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         std::vector<int> visit(n);
         std::iota(visit.begin(), visit.end(), 0);
         std::vector<int> lev;
-        levels_and_order(n, visit, S.lrp, S.lci, lev, S.fwd_order, S.nfwd_levels);
+        levels_and_order(n, visit, S.lrp, S.lci, lev, S.fwd_order, S.nfwd_levels, &S.fwd_lev);
         // Backward levels: row i depends on columns of its U row (all > i).
         std::vector<int> rvisit(n);
         for (int i = 0; i < n; i++) rvisit[i] = n - 1 - i;
-        levels_and_order(n, rvisit, S.urp, S.uci, lev, S.bwd_order, S.nbwd_levels);
+        levels_and_order(n, rvisit, S.urp, S.uci, lev, S.bwd_order, S.nbwd_levels, &S.bwd_lev);
+        // Store the rows contiguously in level order: row fwd_order[idx] of L
+        // occupies [lrp[idx], lrp[idx+1]) (U likewise with bwd_order), so a
+        // sweep streams through memory in the order it consumes it.
+        auto relayout = [n](const std::vector<int>& order, std::vector<int>& rp, std::vector<int>& ci,
+                            std::vector<int>& remap) {
+            std::vector<int> nrp(n + 1, 0), nci(ci.size());
+            remap.assign(ci.size(), -1);
+            for (int idx = 0; idx < n; idx++) {
+                const int i = order[idx];
+                const int len = rp[i + 1] - rp[i];
+                nrp[idx + 1] = nrp[idx] + len;
+                for (int t = 0; t < len; t++) {
+                    nci[nrp[idx] + t] = ci[rp[i] + t];
+                    remap[rp[i] + t] = nrp[idx] + t;
+                }
+            }
+            rp.swap(nrp);
+            ci.swap(nci);
+        };
+        std::vector<int> lmap, umap;
+        relayout(S.fwd_order, S.lrp, S.lci, lmap);
+        relayout(S.bwd_order, S.urp, S.uci, umap);
+        for (int k = 0; k < n; k++) {
+            for (int p = S.cp[k]; p < S.dg[k]; p++) S.slot_dst[p] = umap[S.slot_dst[p]];
+            for (int p = S.dg[k] + 1; p < S.cp[k + 1]; p++) S.slot_dst[p] = lmap[S.slot_dst[p]];
+        }
     }
 
     // Input entries -> slots (column k = invq[c], row = pinv[orig row]).
