@@ -99,6 +99,13 @@ typedef struct {
     int refactor_mode;             /* gathers of dependency columns: 0 staged in
                                       shared memory by asynchronous copies, 1 loaded
                                       per dependency */
+    int inner_prec;                /* A in the inner GMRES products (mixed path):
+                                      0 fp32 values (default), 1 fp64 values (first
+                                      escalation step for ill-conditioned systems) */
+    double xtol;                   /* forward-error target: the refinement stops when
+                                      the residual is <= rtol and the error estimated
+                                      from the last two corrections is <= xtol
+                                      (default 1e-8) */
 } lusp_batch_opts;
 
 /* ---- library ---- */
@@ -165,6 +172,65 @@ int lusp_batch_factor_device_ptr(lusp_batch *b, int sys, void **d_values);
 int lusp_batch_set_params(lusp_batch *b, const lusp_batch_opts *opts);
 /* Kernel launches issued by the last lusp_batch_run (for accounting). */
 int lusp_batch_launch_count(const lusp_batch *b);
+
+/* ---- serving loop ----
+ * Continuous batching of refactor+solve requests from concurrent callers
+ * (Newton steps of Monte-Carlo and corner sweeps).  A scheduler thread keeps
+ * up to `streams` persistent launches in flight; every launch packs the
+ * requests that are ready when a stream frees up (any mix of patterns), so
+ * requests that arrive while others run are admitted as slots free up and
+ * their work overlaps on the device.  Patterns are analysed once on a
+ * separate host thread and kept on the device in an LRU cache keyed by a
+ * hash of (n, Ap, Ai), within hbm_budget_gb together with the launch arenas.
+ * A system whose mixed-precision solve fails (IR stagnation, no
+ * convergence, non-finite, weak or zero pivot) is re-queued once on the
+ * plain fp64 GPU path (LUSP_ST_ESCALATED in its result).  Results do not
+ * depend on what else is in the launch (one CTA runs each system the same
+ * way). */
+typedef struct {
+    lusp_batch_opts solver;        /* prec = LUSP_MIXED (escalating) or LUSP_FP64 */
+    int max_batch;                 /* systems per launch (default 128) */
+    int streams;                   /* launches in flight (default 3) */
+    double hbm_budget_gb;          /* pattern cache + arenas (default 150) */
+    double arena_gb;               /* device arena per stream (default 2) */
+    double staging_mb;             /* pinned host staging per stream (default 256) */
+    int escalate;                  /* re-run failed mixed systems in fp64 (default 1) */
+} lusp_server_opts;
+
+typedef struct {
+    int rc;                        /* LUSP_OK, LUSP_ESINGULAR (analysis), LUSP_EARG */
+    int status;                    /* LUSP_ST_* of the final attempt */
+    double latency_ms;             /* submit -> result available */
+    double queue_ms;               /* submit -> launch */
+    double device_ms;              /* launch that produced the result (device time) */
+    double residual;               /* final ||b - A x|| / ||b|| */
+    int inner_iters, outer_iters, batch_size, cache_hit, escalated, pad_;
+    unsigned long long pattern_hash;
+} lusp_serve_result;
+
+typedef struct {
+    long long submitted, completed, escalated, cache_hits, cache_misses, evictions, launches;
+    long long patterns_resident, max_batch_seen;
+    double pattern_gb;
+} lusp_server_stats;
+
+void lusp_server_opts_default(lusp_server_opts *o);
+int lusp_server_create(const lusp_server_opts *o, lusp_server **out);
+/* Waits for requests in flight, then frees everything. */
+void lusp_server_destroy(lusp_server *s);
+/* Copies the inputs; returns a request id >= 0, or -LUSP_E* on error. */
+long long lusp_serve_submit(lusp_server *s, int n, const int *Ap, const int *Ai, const double *Ax,
+                            const double *b);
+/* wait_ms: 0 poll, > 0 wait at most that long, < 0 wait until done.  Returns
+ * LUSP_OK with x (n doubles, may be NULL) and res filled and the request
+ * released, or LUSP_EBUSY while it runs, or LUSP_EARG for an unknown id. */
+int lusp_serve_poll(lusp_server *s, long long id, double *x, lusp_serve_result *res, int wait_ms);
+int lusp_server_get_stats(lusp_server *s, lusp_server_stats *st);
+
+/* ---- CSR SpMV with fp32 values (fp64 x, y and accumulation); the fp64
+ * version is spmv_launch in spmv.h.  Device pointers. ---- */
+int lusp_csr_spmv32(int n, const int *d_rowptr, const int *d_colidx, const float *d_values,
+                    const double *d_x, double *d_y, void *stream);
 
 /* ---- SELL-C-sigma SpMV (standalone, whole GPU) ---- */
 typedef struct lusp_sell lusp_sell;

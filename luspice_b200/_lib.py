@@ -35,7 +35,28 @@ class BatchOpts(C.Structure):
     _fields_ = [("prec", C.c_int), ("krylov", C.c_int), ("max_outer", C.c_int),
                 ("rtol", C.c_double), ("inner_rel", C.c_double), ("stag_ratio", C.c_double),
                 ("pivot_tol", C.c_double), ("block_threads", C.c_int), ("ctas_per_sm", C.c_int),
-                ("solve_sweep", C.c_int), ("refactor_mode", C.c_int)]
+                ("solve_sweep", C.c_int), ("refactor_mode", C.c_int), ("inner_prec", C.c_int),
+                ("xtol", C.c_double)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("solver", BatchOpts), ("max_batch", C.c_int), ("streams", C.c_int),
+                ("hbm_budget_gb", C.c_double), ("arena_gb", C.c_double), ("staging_mb", C.c_double),
+                ("escalate", C.c_int)]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("rc", C.c_int), ("status", C.c_int), ("latency_ms", C.c_double), ("queue_ms", C.c_double),
+                ("device_ms", C.c_double), ("residual", C.c_double), ("inner_iters", C.c_int),
+                ("outer_iters", C.c_int), ("batch_size", C.c_int), ("cache_hit", C.c_int),
+                ("escalated", C.c_int), ("pad_", C.c_int), ("pattern_hash", C.c_ulonglong)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("escalated", C.c_longlong),
+                ("cache_hits", C.c_longlong), ("cache_misses", C.c_longlong), ("evictions", C.c_longlong),
+                ("launches", C.c_longlong), ("patterns_resident", C.c_longlong),
+                ("max_batch_seen", C.c_longlong), ("pattern_gb", C.c_double)]
 
 
 class DshLuStatic(C.Structure):
@@ -100,6 +121,13 @@ SIGNATURES = {
     "lusp_sell_create": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, C.c_int, C.c_int,
                                    C.c_int, c_void_pp]),
     "lusp_sell_destroy": (None, [C.c_void_p]),
+    "lusp_csr_spmv32": (C.c_int, [C.c_int] + [C.c_void_p] * 6),
+    "lusp_server_opts_default": (None, [C.POINTER(ServerOpts)]),
+    "lusp_server_create": (C.c_int, [C.POINTER(ServerOpts), c_void_pp]),
+    "lusp_server_destroy": (None, [C.c_void_p]),
+    "lusp_serve_submit": (C.c_longlong, [C.c_void_p, C.c_int, c_int_p, c_int_p, c_double_p, c_double_p]),
+    "lusp_serve_poll": (C.c_int, [C.c_void_p, C.c_longlong, c_double_p, C.POINTER(ServeResult), C.c_int]),
+    "lusp_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
     "lusp_sell_spmv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "lusp_sell_info": (C.c_int, [C.c_void_p, c_long_p, c_long_p, c_double_p, c_double_p]),
     # lu_gpu_par.h (C-ABI launchers)

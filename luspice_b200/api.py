@@ -229,6 +229,64 @@ class Sell:
             pass
 
 
+class Server:
+    """Continuous-batching request loop (lusp_server_*)."""
+
+    def __init__(self, prec: int = MIXED, **opts):
+        lib = L.load()
+        o = L.ServerOpts()
+        lib.lusp_server_opts_default(C.byref(o))
+        o.solver.prec = prec
+        for k, v in opts.items():
+            if hasattr(o, k):
+                setattr(o, k, v)
+            elif hasattr(o.solver, k):
+                setattr(o.solver, k, v)
+            else:
+                raise TypeError(f"unknown server option {k}")
+        h = C.c_void_p()
+        _check(lib.lusp_server_create(C.byref(o), C.byref(h)), "lusp_server_create")
+        self.handle = h
+        self.sizes = {}
+
+    def submit(self, n, Ap, Ai, Ax, b) -> int:
+        Ap, Ai, Ax, b = _i32(Ap), _i32(Ai), _f64(Ax), _f64(b)
+        rid = L.load().lusp_serve_submit(self.handle, int(n), L.ptr(Ap, C.c_int), L.ptr(Ai, C.c_int),
+                                         L.ptr(Ax, C.c_double), L.ptr(b, C.c_double))
+        if rid < 0:
+            raise LuspError(-rid, "lusp_serve_submit")
+        self.sizes[rid] = int(n)
+        return rid
+
+    def poll(self, rid: int, wait_ms: int = -1):
+        """(x, result dict) when done, None while running."""
+        n = self.sizes[rid]
+        x = np.empty(n)
+        r = L.ServeResult()
+        rc = L.load().lusp_serve_poll(self.handle, rid, L.ptr(x, C.c_double), C.byref(r), wait_ms)
+        if rc == 6:
+            return None
+        _check(rc, "lusp_serve_poll")
+        del self.sizes[rid]
+        return x, {k: getattr(r, k) for k, _ in L.ServeResult._fields_ if k != "pad_"}
+
+    def stats(self) -> dict:
+        st = L.ServerStats()
+        _check(L.load().lusp_server_get_stats(self.handle, C.byref(st)), "stats")
+        return {k: getattr(st, k) for k, _ in L.ServerStats._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            L.load().lusp_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def colamd(n: int, Ap, Ai, knob_row: float = 0.0, knob_col: float = 0.0) -> np.ndarray:
     Ap, Ai = _i32(Ap), _i32(Ai)
     q = np.empty(n, np.int32)

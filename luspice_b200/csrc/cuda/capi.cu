@@ -150,6 +150,8 @@ void lusp_batch_opts_default(lusp_batch_opts* o) {
     o->ctas_per_sm = 2;
     o->solve_sweep = 0;
     o->refactor_mode = 0;
+    o->inner_prec = 0;
+    o->xtol = 1e-8;
 }
 
 int lusp_batch_create(int nsys, lusp_pattern* const* pats, const lusp_batch_opts* opts,
@@ -289,6 +291,8 @@ int lusp_batch_set_params(lusp_batch* hb, const lusp_batch_opts* o) {
     B->prm.inner_rel = o->inner_rel;
     B->prm.stag_ratio = o->stag_ratio;
     B->prm.pivot_tol = o->pivot_tol;
+    B->prm.xtol = o->xtol > 0 ? o->xtol : 1e-8;
+    B->launch.prm = B->prm;
     // Captured graphs hold the old parameters by value.
     for (auto& kv : B->graphs) {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);

@@ -71,9 +71,11 @@ batch_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan
 // ---------------------------------------------------------------------------
 // Patterns
 // ---------------------------------------------------------------------------
-static int upload_ints(const std::vector<int>& v, int* dst, cudaStream_t st) {
+// Synchronous copy from pageable memory: returns when the data is on the
+// device, without waiting for kernels on other (non-blocking) streams.
+static int upload_ints(const std::vector<int>& v, int* dst, cudaStream_t) {
     if (v.empty()) return 0;
-    cudaError_t e = cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaError_t e = cudaMemcpy(dst, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice);
     return e == cudaSuccess ? 0 : cuda_fail(e, "pattern upload");
 }
 
@@ -185,8 +187,6 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     if (e != cudaSuccess) { pattern_free(P); return cuda_fail(e, "pattern descriptor alloc"); }
     e = cudaMemcpy(P->d_desc, &D, sizeof(PatternDev), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { pattern_free(P); return cuda_fail(e, "pattern descriptor upload"); }
-    e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) { pattern_free(P); return cuda_fail(e, "pattern upload sync"); }
     *out = P;
     return LUSP_OK;
 }
@@ -201,7 +201,7 @@ void pattern_free(PatternObj* P) {
 // ---------------------------------------------------------------------------
 // Batches
 // ---------------------------------------------------------------------------
-static int sm_count() {
+int sm_count() {
     static int cached = 0;
     if (!cached) {
         int dev = 0;
@@ -258,35 +258,114 @@ void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm,
     plan.bytes = fixed + std::max(solve_bytes, ref_bytes);
 }
 
+// Raise the dynamic shared-memory limit of one kernel instantiation (once
+// per size; not a stream operation, so it stays out of captured graphs after
+// the first call) and optionally report its occupancy.
 template <typename VT, typename AT>
-static int launch_typed(BatchObj* B, int what, cudaStream_t st) {
+static int kernel_prepare(size_t smem, int block, int* occ) {
     auto kern = batch_kernel<VT, AT>;
-    // Raise the dynamic shared-memory limit once per size (not a stream
-    // operation, so it stays out of captured graphs after the first call).
     static std::mutex mu;
     static size_t granted = 0;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (B->plan.bytes > granted) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->plan.bytes);
-            if (e != cudaSuccess) return cuda_fail(e, "kernel smem attribute");
-            granted = B->plan.bytes;
-        }
+    std::lock_guard<std::mutex> lk(mu);
+    if (smem > granted) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "kernel smem attribute");
+        granted = smem;
     }
-    cudaError_t e = cudaMemsetAsync(B->d_queue, 0, sizeof(int), st);
-    if (e != cudaSuccess) return cuda_fail(e, "queue reset");
-    const int direct = (B->prec == LUSP_FP64 || (what & LUSP_RUN_DIRECT)) ? 1 : 0;
-    kern<<<B->grid, B->block, B->plan.bytes, st>>>(B->d_sys, B->nsys, B->d_queue, B->plan, B->prm,
-                                                  what & 3, direct);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "batch kernel launch");
-    B->launches = 1;
+    if (occ) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, block, smem);
+        if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+    }
     return LUSP_OK;
 }
 
+int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ) {
+    if (prec == LUSP_FP64) return kernel_prepare<double, double>(smem, block, occ);
+    if (inner == 1) return kernel_prepare<float, double>(smem, block, occ);
+    return kernel_prepare<float, float>(smem, block, occ);
+}
+
+template <typename VT, typename AT>
+static int launch_typed(const LaunchArgs& a, cudaStream_t st) {
+    int rc = kernel_prepare<VT, AT>(a.plan.bytes, a.block, nullptr);
+    if (rc != LUSP_OK) return rc;
+    cudaError_t e = cudaMemsetAsync(a.d_queue, 0, sizeof(int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "queue reset");
+    const int direct = (a.prec == LUSP_FP64 || (a.what & LUSP_RUN_DIRECT)) ? 1 : 0;
+    batch_kernel<VT, AT><<<a.grid, a.block, a.plan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.plan, a.prm,
+                                                              a.what & 3, direct);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "batch kernel launch");
+    return LUSP_OK;
+}
+
+int launch_systems(const LaunchArgs& a, cudaStream_t st) {
+    if (a.prec == LUSP_FP64) return launch_typed<double, double>(a, st);
+    if (a.inner == 1) return launch_typed<float, double>(a, st);
+    return launch_typed<float, float>(a, st);
+}
+
 int batch_launch(BatchObj* B, int what, cudaStream_t st) {
-    if (B->prec == LUSP_FP64) return launch_typed<double, double>(B, what, st);
-    return launch_typed<float, float>(B, what, st);
+    LaunchArgs a = B->launch;
+    a.what = what;
+    int rc = launch_systems(a, st);
+    if (rc == LUSP_OK) B->launches = 1;
+    return rc;
+}
+
+static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t system_private_bytes(const StaticPattern& S, size_t vs, int m) {
+    const size_t n = S.n;
+    const size_t st = S.sell_ptr.back();
+    return al256(S.cap * vs) + al256(S.lci.size() * vs) + al256(S.uci.size() * vs) + al256(n * vs) +
+           al256(st * 8) + al256(st * 4) + al256(((size_t)m + 8) * n * 8);
+}
+
+char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m) {
+    const size_t n = S.n;
+    const size_t st = S.sell_ptr.back();
+    D.lu = p; p += al256(S.cap * vs);
+    D.lval = p; p += al256(S.lci.size() * vs);
+    D.uval = p; p += al256(S.uci.size() * vs);
+    D.udiag = p; p += al256(n * vs);
+    D.sell64 = (double*)p; p += al256(st * 8);
+    D.sell32 = (float*)p; p += al256(st * 4);
+    D.work = (double*)p; p += al256(((size_t)m + 8) * n * 8);
+    return p;
+}
+
+size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& plan) {
+    return colmax > plan.wcap ? al256((size_t)grid * (block / 32) * colmax * 8) : 0;
+}
+
+int check_opts(const lusp_batch_opts* o) {
+    if (o->prec != LUSP_MIXED && o->prec != LUSP_FP64) { set_error("bad prec"); return LUSP_EARG; }
+    if (o->krylov < 1 || o->krylov > kMaxKrylov) { set_error("krylov must be 1..%d", kMaxKrylov); return LUSP_EARG; }
+    if (o->block_threads < 64 || o->block_threads > 512 || o->block_threads % 32) { set_error("block_threads must be 64..512, a multiple of 32"); return LUSP_EARG; }
+    if (o->inner_prec < 0 || o->inner_prec > 1) { set_error("bad inner_prec"); return LUSP_EARG; }
+    return LUSP_OK;
+}
+
+void fill_params(SolveParams& prm, const lusp_batch_opts& o) {
+    prm.m = o.krylov;
+    prm.max_outer = std::max(0, o.max_outer);
+    prm.rtol = o.rtol;
+    prm.inner_rel = o.inner_rel;
+    prm.stag_ratio = o.stag_ratio;
+    prm.pivot_tol = o.pivot_tol;
+    prm.refactor_mode = o.refactor_mode;
+    prm.xtol = o.xtol > 0 ? o.xtol : 1e-8;
+}
+
+int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, SmemPlan& plan) {
+    make_plan(pats, o.block_threads, o.ctas_per_sm, o.krylov, o.prec == LUSP_FP64 ? 8 : 4, plan);
+    if (o.solve_sweep == 1) plan.dcap = 0;   // dataflow sweeps only
+    if (o.solve_sweep == 2 && plan.dcap == 0) {
+        set_error("level-synchronous sweeps need the solve vector and descriptors in shared memory");
+        return LUSP_EARG;
+    }
+    return LUSP_OK;
 }
 
 int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, BatchObj** out) {
@@ -294,32 +373,19 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     if (nsys <= 0 || !pats || !o) { set_error("batch_create: bad arguments"); return LUSP_EARG; }
     for (int s = 0; s < nsys; s++)
         if (!pats[s]) { set_error("batch_create: null pattern %d", s); return LUSP_EARG; }
-    if (o->prec != LUSP_MIXED && o->prec != LUSP_FP64) { set_error("batch_create: bad prec"); return LUSP_EARG; }
-    if (o->krylov < 1 || o->krylov > kMaxKrylov) { set_error("batch_create: krylov must be 1..%d", kMaxKrylov); return LUSP_EARG; }
-    if (o->block_threads < 64 || o->block_threads > 512 || o->block_threads % 32) { set_error("batch_create: block_threads"); return LUSP_EARG; }
+    int rc = check_opts(o);
+    if (rc != LUSP_OK) return rc;
     BatchObj* B = new BatchObj();
     B->nsys = nsys;
     B->prec = o->prec;
     B->opts = *o;
     B->pats.assign(pats, pats + nsys);
     B->block = o->block_threads;
-    B->prm.m = o->krylov;
-    B->prm.max_outer = std::max(0, o->max_outer);
-    B->prm.rtol = o->rtol;
-    B->prm.inner_rel = o->inner_rel;
-    B->prm.stag_ratio = o->stag_ratio;
-    B->prm.pivot_tol = o->pivot_tol;
-    B->prm.refactor_mode = o->refactor_mode;
-    make_plan(B->pats, B->block, o->ctas_per_sm, o->krylov, B->prec == LUSP_FP64 ? 8 : 4, B->plan);
-    if (o->solve_sweep == 1) B->plan.dcap = 0;   // dataflow sweeps only
-    if (o->solve_sweep == 2 && B->plan.dcap == 0) {
-        set_error("batch_create: level-synchronous sweeps need the solve vector and descriptors in shared memory");
-        delete B;
-        return LUSP_EARG;
-    }
+    fill_params(B->prm, *o);
+    rc = plan_for(B->pats, *o, B->plan);
+    if (rc != LUSP_OK) { delete B; return rc; }
 
     const size_t vs = B->prec == LUSP_FP64 ? 8 : 4;
-    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     // Inputs and outputs of all systems are contiguous (values, rhs, x) so a
     // batch moves host<->device in one copy each; the rest is per system.
     std::vector<size_t> base(nsys + 1, 0);
@@ -329,40 +395,19 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
         B->val_off[s + 1] = B->val_off[s] + B->pats[s]->S.nnz_a;
         B->vec_off[s + 1] = B->vec_off[s] + B->pats[s]->S.n;
     }
-    const size_t io_bytes = al(B->val_off[nsys] * 8) + 2 * al(B->vec_off[nsys] * 8);
-    base[0] = io_bytes;
-    for (int s = 0; s < nsys; s++) {
-        const StaticPattern& S = B->pats[s]->S;
-        const size_t n = S.n;
-        const size_t st = S.sell_ptr.back();
-        size_t b = 0;
-        b += al(S.cap * vs);                        // lu
-        b += al(S.lci.size() * vs);                 // lval
-        b += al(S.uci.size() * vs);                 // uval
-        b += al(n * vs);                            // udiag
-        b += al(st * 8) + al(st * 4);               // sell64, sell32
-        b += al(((size_t)o->krylov + 8) * n * 8);   // work
-        base[s + 1] = base[s] + b;
-    }
-    // Spill area for columns longer than the shared-memory work area.
+    base[0] = al256(B->val_off[nsys] * 8) + 2 * al256(B->vec_off[nsys] * 8);
+    for (int s = 0; s < nsys; s++) base[s + 1] = base[s] + system_private_bytes(B->pats[s]->S, vs, o->krylov);
     int colmax = 0;
     for (auto* p : B->pats) colmax = std::max(colmax, p->S.max_col);
     int occ = 0;
-    cudaError_t e;
-    if (B->prec == LUSP_FP64) {
-        cudaFuncSetAttribute(batch_kernel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->plan.bytes);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel<double, double>, B->block, B->plan.bytes);
-    } else {
-        cudaFuncSetAttribute(batch_kernel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->plan.bytes);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel<float, float>, B->block, B->plan.bytes);
-    }
-    if (e != cudaSuccess) { delete B; return cuda_fail(e, "occupancy query"); }
+    rc = kernel_occupancy(B->prec, o->inner_prec, B->plan.bytes, B->block, &occ);
+    if (rc != LUSP_OK) { delete B; return rc; }
     if (occ < 1) { delete B; set_error("batch_create: kernel does not fit one SM (smem %zu)", B->plan.bytes); return LUSP_EARG; }
     B->grid = std::min(nsys, occ * sm_count());
-    const size_t spill = colmax > B->plan.wcap ? al((size_t)B->grid * (B->block / 32) * colmax * 8) : 0;
-    const size_t total = base[nsys] + spill + al(sizeof(SysStats) * nsys) + al(sizeof(SysDev) * nsys) + 256;
+    const size_t spill = spill_bytes(B->grid, B->block, colmax, B->plan);
+    const size_t total = base[nsys] + spill + al256(sizeof(SysStats) * nsys) + al256(sizeof(SysDev) * nsys) + 256;
     char* blk = nullptr;
-    e = cudaMalloc(&blk, total);
+    cudaError_t e = cudaMalloc(&blk, total);
     if (e != cudaSuccess) { delete B; return cuda_fail(e, "batch device alloc"); }
     B->d_block = blk;
     B->bytes = total;
@@ -370,35 +415,36 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     if (e != cudaSuccess) { batch_free(B); return cuda_fail(e, "batch memset"); }
     char* stats_base = blk + base[nsys] + spill;
     B->d_stats = (SysStats*)stats_base;
-    B->d_sys = (SysDev*)(stats_base + al(sizeof(SysStats) * nsys));
-    B->d_queue = (int*)((char*)B->d_sys + al(sizeof(SysDev) * nsys));
+    B->d_sys = (SysDev*)(stats_base + al256(sizeof(SysStats) * nsys));
+    B->d_queue = (int*)((char*)B->d_sys + al256(sizeof(SysDev) * nsys));
     double* spill_ptr = spill ? (double*)(blk + base[nsys]) : nullptr;
     B->d_vals = (double*)blk;
-    B->d_rhs = (double*)(blk + al(B->val_off[nsys] * 8));
-    B->d_x = (double*)(blk + al(B->val_off[nsys] * 8) + al(B->vec_off[nsys] * 8));
+    B->d_rhs = (double*)(blk + al256(B->val_off[nsys] * 8));
+    B->d_x = (double*)(blk + al256(B->val_off[nsys] * 8) + al256(B->vec_off[nsys] * 8));
     B->h_sys.resize(nsys);
     for (int s = 0; s < nsys; s++) {
-        const StaticPattern& S = B->pats[s]->S;
-        const size_t n = S.n;
-        const size_t st = S.sell_ptr.back();
-        char* p = blk + base[s];
         SysDev& D = B->h_sys[s];
         D.pat = B->pats[s]->d_desc;
         D.a_val = B->d_vals + B->val_off[s];
         D.b = B->d_rhs + B->vec_off[s];
         D.x = B->d_x + B->vec_off[s];
-        D.lu = p; p += al(S.cap * vs);
-        D.lval = p; p += al(S.lci.size() * vs);
-        D.uval = p; p += al(S.uci.size() * vs);
-        D.udiag = p; p += al(n * vs);
-        D.sell64 = (double*)p; p += al(st * 8);
-        D.sell32 = (float*)p; p += al(st * 4);
-        D.work = (double*)p; p += al(((size_t)o->krylov + 8) * n * 8);
+        carve_system(D, blk + base[s], B->pats[s]->S, vs, o->krylov);
         D.scratch = spill_ptr;
         D.stats = B->d_stats + s;
     }
     e = cudaMemcpy(B->d_sys, B->h_sys.data(), sizeof(SysDev) * nsys, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { batch_free(B); return cuda_fail(e, "batch descriptor upload"); }
+    LaunchArgs& a = B->launch;
+    a.d_sys = B->d_sys;
+    a.nsys = nsys;
+    a.d_queue = B->d_queue;
+    a.plan = B->plan;
+    a.prm = B->prm;
+    a.prec = B->prec;
+    a.inner = o->inner_prec;
+    a.what = LUSP_RUN_BOTH;
+    a.block = B->block;
+    a.grid = B->grid;
     *out = B;
     return LUSP_OK;
 }

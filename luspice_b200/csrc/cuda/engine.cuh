@@ -86,6 +86,7 @@ struct SolveParams {
     double stag_ratio;       // residual must shrink by this factor per outer
     double pivot_tol;        // frozen-pivot acceptance threshold
     int refactor_mode;       // 0 staged gathers (cp.async), 1 per-dependency loads
+    double xtol;             // forward-error target of the refinement
 };
 
 constexpr int kMaxKrylov = 64;

@@ -21,6 +21,21 @@ struct PatternObj {
     size_t bytes = 0;
 };
 
+// Everything one persistent launch needs (device descriptors already
+// uploaded).
+struct LaunchArgs {
+    const SysDev* d_sys = nullptr;
+    int nsys = 0;
+    int* d_queue = nullptr;
+    SmemPlan plan{};
+    SolveParams prm{};
+    int prec = LUSP_MIXED;
+    int inner = 0;
+    int what = LUSP_RUN_BOTH;
+    int block = 256;
+    int grid = 1;
+};
+
 struct GraphEntry {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -46,6 +61,7 @@ struct BatchObj {
     int block = 256;
     int grid = 1;
     int launches = 0;
+    LaunchArgs launch{};
     std::map<std::pair<int, cudaStream_t>, GraphEntry> graphs;
 };
 
@@ -59,6 +75,17 @@ void pattern_free(PatternObj* P);
 void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm, int m, int vsize,
                SmemPlan& plan);
 int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, BatchObj** out);
+
+// Building blocks shared by batches and the serving loop.
+int check_opts(const lusp_batch_opts* o);
+void fill_params(SolveParams& prm, const lusp_batch_opts& o);
+int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, SmemPlan& plan);
+int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ);
+size_t system_private_bytes(const StaticPattern& S, size_t vs, int m);
+char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m);
+size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& plan);
+int launch_systems(const LaunchArgs& a, cudaStream_t st);
+int sm_count();
 void batch_free(BatchObj* B);
 int batch_launch(BatchObj* B, int what, cudaStream_t st);
 

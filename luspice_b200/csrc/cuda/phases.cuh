@@ -611,7 +611,7 @@ __device__ void direct_phase(const SysDev& S, const SmemPlan& plan, char* smem_b
 // factors as preconditioner (VT), inner products A z with AT values; outer
 // residual b - A x, Arnoldi (classical Gram-Schmidt, two passes), Givens
 // rotations, least-squares update and solution update in fp64.
-// Workspace (doubles): bt, xt, r, z, w, yg (n each), V ((m+1) n).
+// Workspace (doubles): bt, xt, r, z, w, yg (n each), V ((m+1) n), xprev (n).
 // ---------------------------------------------------------------------------
 template <typename VT, typename AT>
 __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_base,
@@ -628,6 +628,7 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
     double* w = z + n;
     double* yg = w + n;
     double* V = yg + n;
+    double* xprev = V + (size_t)(m + 1) * n;   // iterate before the last correction
     // Shared: y (optional) | H[(m+1) x m] | g, cs, sn, h, h2, yc
     double* ys = (double*)sm.uni;
     double* H = ys + plan.ycap;
@@ -669,6 +670,10 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         return;
     }
     double res_prev = INFINITY;
+    // Forward-error estimate of the current iterate from the last two
+    // corrections: contraction rho = |dx_k| / |dx_k-1|, remaining error
+    // ~ |dx_k| rho / (1 - rho) relative to |x|.
+    double dx_prev = 0.0, err_est = INFINITY;
     for (int outer = 0;; outer++) {
         if (outer == 0) {
             for (int i = threadIdx.x; i < n; i += blockDim.x) r[i] = bt[i];
@@ -682,8 +687,18 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
             if (threadIdx.x == 0) S.stats->res[nres] = res;
             nres++;
         }
+        // A correction that made the residual worse (or non-finite) is
+        // undone: the result is the best iterate, the status says why.
+        if (outer > 0 && !(res <= res_prev)) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) xt[i] = xprev[i];
+            __syncthreads();
+            status |= isfinite(res) ? ST_STAGNATED : ST_NONFINITE;
+            break;
+        }
         if (!isfinite(res)) { status |= ST_NONFINITE; break; }
-        if (res <= prm.rtol) break;
+        // Converged when the residual is small and the iterate has stopped
+        // moving (or the residual is at fp64 round-off, nothing left to gain).
+        if (res <= prm.rtol && (err_est <= prm.xtol || res <= 1e-15)) break;
         if (outer >= prm.max_outer) { status |= ST_NOT_CONVERGED; break; }
         if (outer > 0 && res > prm.stag_ratio * res_prev) { status |= ST_STAGNATED; break; }
         res_prev = res;
@@ -693,7 +708,9 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
             for (int t = 0; t <= m; t++) g[t] = 0.0;
             g[0] = beta;
         }
-        const double inner_stop = fmax(prm.rtol * nb, prm.inner_rel * beta);
+        // Inner solve: reduce the current residual by inner_rel (a cap at
+        // rtol * |b| would stall the outer loop right above rtol).
+        const double inner_stop = prm.inner_rel * beta;
         int jj = 0;
         for (int j = 0; j < m; j++) {
             const double* vj = V + (size_t)j * n;
@@ -767,8 +784,22 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         }
         __syncthreads();
         lu_apply<VT>(P, lval, uval, udiag, z, y, sm, desc, bad);
-        for (int e = threadIdx.x; e < n; e += blockDim.x) xt[e] += y[e];
-        __syncthreads();
+        double sy = 0.0, sx = 0.0;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            xprev[e] = xt[e];
+            const double xn = xt[e] + y[e];
+            xt[e] = xn;
+            sy = fma(y[e], y[e], sy);
+            sx = fma(xn, xn, sx);
+        }
+        const double ny = sqrt(block_sum(sy, sm.red));
+        const double nx = sqrt(block_sum(sx, sm.red));
+        const double dx = nx > 0.0 ? ny / nx : ny;
+        if (dx_prev > 0.0) {
+            const double rho = fmin(dx / dx_prev, 0.99);
+            err_est = dx * rho / (1.0 - rho);
+        }
+        dx_prev = dx;
         outer_done++;
     }
     for (int i = threadIdx.x; i < n; i += blockDim.x) S.x[P.q[i]] = xt[i];

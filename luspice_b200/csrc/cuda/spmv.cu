@@ -27,16 +27,18 @@ namespace {
 
 constexpr int kCsrLanes = 4;
 
+template <typename VT>
 __global__ void __launch_bounds__(256)
 csr_vector_kernel(int n, const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                  const double* __restrict__ values, const double* __restrict__ x,
+                  const VT* __restrict__ values, const double* __restrict__ x,
                   double* __restrict__ y) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / kCsrLanes;
     const int sub = threadIdx.x % kCsrLanes;
     double acc = 0.0;
     if (g < n) {
         const int p1 = rowptr[g + 1];
-        for (int p = rowptr[g] + sub; p < p1; p += kCsrLanes) acc = fma(values[p], __ldg(x + colidx[p]), acc);
+        for (int p = rowptr[g] + sub; p < p1; p += kCsrLanes)
+            acc = fma((double)values[p], __ldg(x + colidx[p]), acc);
     }
 #pragma unroll
     for (int o = kCsrLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -149,7 +151,17 @@ void spmv_launch(int n, const int* d_rowptr, const int* d_colidx, const double* 
     if (n <= 0) return;
     const long threads = (long)n * kCsrLanes;
     const int grid = (int)((threads + 255) / 256);
-    csr_vector_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(n, d_rowptr, d_colidx, d_values, d_x, d_y);
+    csr_vector_kernel<double><<<grid, 256, 0, (cudaStream_t)stream>>>(n, d_rowptr, d_colidx, d_values, d_x, d_y);
+}
+
+int lusp_csr_spmv32(int n, const int* d_rowptr, const int* d_colidx, const float* d_values,
+                    const double* d_x, double* d_y, void* stream) {
+    if (n <= 0 || !d_rowptr || !d_colidx || !d_values || !d_x || !d_y) return LUSP_EARG;
+    const long threads = (long)n * kCsrLanes;
+    const int grid = (int)((threads + 255) / 256);
+    csr_vector_kernel<float><<<grid, 256, 0, (cudaStream_t)stream>>>(n, d_rowptr, d_colidx, d_values, d_x, d_y);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LUSP_OK : lusp::cuda_fail(e, "csr fp32 spmv launch");
 }
 
 int spmv_host(const CSRMatrix* A, const double* x, double* y, double* time_ms) {

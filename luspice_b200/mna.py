@@ -294,6 +294,27 @@ def large_circuit(n_total: int = 40000, seed: int = 42, supply_nets: int = 4,
     return m
 
 
+def ill_conditioned(m: MNAMatrix, seed: int, width: int = 8, scale: float = 1e-14) -> np.ndarray:
+    """Values of an ill-conditioned Newton step on m's pattern: every element
+    touching one subcircuit (a window of `width` node rows) is scaled by
+    `scale`, and one further node keeps only its gmin (all its other
+    elements are scaled by 1e-30)."""
+    rng = np.random.default_rng(seed)
+    nodes = int(m.meta.get("nodes", m.n))
+    i0 = int(rng.integers(0, max(1, nodes - width - 1)))
+    rows = np.repeat(np.arange(m.nnz), np.diff(m.stamp.indptr))
+    elems = m.stamp.indices
+    entry_row = m.Ai[rows]
+    fac = np.ones(m.elem_val.size)
+    touch = np.unique(elems[(entry_row >= i0) & (entry_row < i0 + width)])
+    fac[touch] = scale
+    lone = i0 + width
+    gmin = m.elem_val == 1e-12
+    touch2 = np.unique(elems[entry_row == lone])
+    fac[touch2[~gmin[touch2]]] = 1e-30
+    return m.values(fac)
+
+
 def batch_sizes(count: int = 512, lo: int = 100, hi: int = 5000, seed: int = 42) -> np.ndarray:
     """Matrix sizes of the uneven batch: n ~ U[lo, hi] from the base seed."""
     return np.random.default_rng(seed).integers(lo, hi + 1, count)

@@ -126,3 +126,37 @@ def test_sell_fp16_ruiz(gpu):
     ref = A @ x
     # fp16 storage: relative error of each product <= 2^-11.
     assert np.all(np.abs(dy.cpu().numpy() - ref) <= 2.0 ** -10 * (np.abs(A) @ np.abs(x)) + 1e-300)
+
+
+def test_csr_spmv32(gpu, lib):
+    import torch
+    m = mna.analog(3000, 6)
+    A = m.csr()
+    x = np.random.default_rng(3).standard_normal(m.n)
+    rp, ci = _dev(torch, A.indptr, torch.int32), _dev(torch, A.indices, torch.int32)
+    v32 = _dev(torch, A.data.astype(np.float32), torch.float32)
+    dx, dy = _dev(torch, x, torch.float64), torch.zeros(m.n, dtype=torch.float64, device="cuda")
+    assert lib.lusp_csr_spmv32(m.n, _p(rp), _p(ci), _p(v32), _p(dx), _p(dy), None) == 0
+    torch.cuda.synchronize()
+    ref = sp.csr_matrix((A.data.astype(np.float32).astype(np.float64), A.indices, A.indptr), shape=A.shape) @ x
+    assert np.all(np.abs(dy.cpu().numpy() - ref) <= 1e-12 * (np.abs(A) @ np.abs(x)) + 1e-300)
+
+
+def test_large_circuit_spmv_variants(gpu, lib):
+    """n = 40,000 with supply rows: fp64/fp32 CSR and SELL agree with the host
+    product; fp16 is refused because the scaled range does not fit."""
+    import torch
+    m = mna.large_circuit()
+    A = m.csr()
+    x = np.random.default_rng(4).standard_normal(m.n)
+    ref = A @ x
+    scale = np.abs(A) @ np.abs(x)
+    dx = _dev(torch, x, torch.float64)
+    for kind, tol in (("fp64", 1e-13), ("fp32", 1e-6)):
+        S = api.Sell(m.n, A.indptr, A.indices, A.data, 32, 256, kind)
+        dy = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+        S.spmv(dx.data_ptr(), dy.data_ptr())
+        torch.cuda.synchronize()
+        assert np.all(np.abs(dy.cpu().numpy() - ref) <= tol * scale + 1e-300), kind
+    with pytest.raises(api.LuspError):
+        api.Sell(m.n, A.indptr, A.indices, A.data, 32, 256, "fp16")

@@ -1,0 +1,95 @@
+"""Serving loop: continuous batching, pattern cache, escalation, and the
+same result alone and in a mix."""
+import threading
+
+import numpy as np
+import pytest
+
+from luspice_b200 import api, mna
+from tests.helpers import TOL_REL, oracle_solution, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def test_same_result_alone_and_in_mix(gpu):
+    m = mna.analog(989, 42)
+    vals = m.perturbed(1, seed=9)[0]
+    S = api.Server(max_batch=64, streams=3, arena_gb=1.0, staging_mb=64)
+    rid = S.submit(m.n, m.Ap, m.Ai, vals, m.b)
+    x_alone, r_alone = S.poll(rid, 120000)
+    assert r_alone["rc"] == 0 and r_alone["batch_size"] == 1
+    # Now the same system among 60 others of 4 patterns, from two threads.
+    others = [mna.analog(int(n), 100 + i) for i, n in enumerate([300, 1500, 700, 2500])]
+    ids, lock = [], threading.Lock()
+
+    def worker(k):
+        for t in range(30):
+            mm = others[(t + k) % len(others)]
+            v = mm.perturbed(1, seed=1000 * k + t)[0]
+            i = S.submit(mm.n, mm.Ap, mm.Ai, v, mm.b)
+            with lock:
+                ids.append((i, mm, v))
+            if t == 15 and k == 0:
+                j = S.submit(m.n, m.Ap, m.Ai, vals, m.b)
+                with lock:
+                    ids.append((j, None, None))
+
+    th = [threading.Thread(target=worker, args=(k,)) for k in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    mixed = None
+    batch_sizes = []
+    for i, mm, v in ids:
+        x, r = S.poll(i, 120000)
+        assert r["rc"] == 0, r
+        batch_sizes.append(r["batch_size"])
+        if mm is None:
+            mixed = (x, r)
+        else:
+            assert r["residual"] <= 1e-10, r
+            assert rel_err(x, oracle_solution(mm, v)) <= TOL_REL
+    x_mixed, r_mixed = mixed
+    assert np.array_equal(x_alone, x_mixed), (np.abs(x_alone - x_mixed).max(), r_alone, r_mixed)
+    assert rel_err(x_mixed, oracle_solution(m, vals)) <= TOL_REL
+    st = S.stats()
+    assert st["cache_hits"] >= 55 and st["cache_misses"] == 5
+    assert max(batch_sizes) > 1          # requests were batched together
+    S.close()
+
+
+def test_escalation_to_fp64(gpu):
+    m = mna.analog(989, 42)
+    bad = mna.ill_conditioned(m, seed=3)
+    S = api.Server(max_batch=16, streams=2, arena_gb=0.5, staging_mb=32)
+    i_ok = S.submit(m.n, m.Ap, m.Ai, m.Ax, m.b)
+    i_bad = S.submit(m.n, m.Ap, m.Ai, bad, m.b)
+    x_ok, r_ok = S.poll(i_ok, 120000)
+    x_bad, r_bad = S.poll(i_bad, 120000)
+    assert r_ok["rc"] == 0 and not r_ok["escalated"]
+    assert rel_err(x_ok, m.x_true) <= TOL_REL
+    assert r_bad["rc"] == 0
+    from luspice_b200 import api as A
+    if r_bad["escalated"]:
+        assert r_bad["status"] & A.ST_ESCALATED
+    # Whatever path it took, the answer is the fp64 oracle's.
+    from luspice_b200.api import Pattern
+    P = Pattern.from_matrix(m)
+    _, q = P.perm()
+    ref = oracle_solution(m, bad, q=q)
+    r = np.linalg.norm(m.matvec(x_bad, bad) - m.b) / np.linalg.norm(m.b)
+    r_ref = np.linalg.norm(m.matvec(ref, bad) - m.b) / np.linalg.norm(m.b)
+    assert r <= max(10 * r_ref, 1e-9), (r, r_ref, r_bad)
+    S.close()
+
+
+def test_singular_pattern_reported(gpu):
+    S = api.Server(max_batch=4, streams=1, arena_gb=0.25, staging_mb=16)
+    Ap = np.array([0, 2, 4, 5], np.int32)
+    Ai = np.array([0, 1, 0, 1, 2], np.int32)
+    Ax = np.array([1.0, 2.0, 2.0, 4.0, 1.0])
+    rid = S.submit(3, Ap, Ai, Ax, np.ones(3))
+    _, r = S.poll(rid, 120000)
+    assert r["rc"] == 1
+    S.close()
