@@ -72,6 +72,8 @@ typedef struct {
     unsigned long long hash;
     size_t device_bytes;
     int singular_col;              /* -1 unless creation failed as singular */
+    int dense_tail;                /* columns of the dense trailing block (0: none) */
+    int tail_start;                /* its first position (n when there is none) */
 } lusp_pattern_info;
 
 typedef struct {
@@ -81,6 +83,12 @@ typedef struct {
     /* SM cycles summed over warps: refactor waits for dependency columns,
      * gathers of their L parts, updates; refactor wall cycles of the CTA */
     long long cyc_wait, cyc_gather, cyc_update, cyc_refactor;
+    /* SM cycles of the solve phase (CTA wall time): L sweeps, dense-tail
+     * solves, U sweeps, SpMVs, the whole solve */
+    long long cyc_lsolve, cyc_tail, cyc_usolve, cyc_spmv, cyc_solve;
+    /* SM cycles of the refactor's dense trailing block: panels, U-row
+     * solves, trailing updates */
+    long long cyc_tpanel, cyc_ttrsm, cyc_tupdate;
 } lusp_sys_stats;
 
 typedef struct {
@@ -91,14 +99,15 @@ typedef struct {
     double inner_rel;              /* inner stop vs current residual (default 1e-8) */
     double stag_ratio;             /* required residual reduction per outer (default 0.5) */
     double pivot_tol;              /* frozen-pivot acceptance (default 1e-3) */
-    int block_threads;             /* CTA size (default 256) */
-    int ctas_per_sm;               /* shared-memory plan target (default 2) */
+    int block_threads;             /* CTA size of the solve kernel (default 256) */
+    int ctas_per_sm;               /* solve kernel shared-memory plan target (default 2) */
     int solve_sweep;               /* triangular solves: 0 auto, 1 dataflow (per-row
                                       ready bits), 2 level-synchronous (barrier per
                                       level, descriptors in shared memory) */
     int refactor_mode;             /* gathers of dependency columns: 0 staged in
-                                      shared memory by asynchronous copies, 1 loaded
-                                      per dependency */
+                                      shared memory by asynchronous copies with
+                                      precomputed relative slots, 1 loaded per
+                                      dependency with a search of the column's rows */
     int inner_prec;                /* A in the inner GMRES products (mixed path):
                                       0 fp32 values (default), 1 fp64 values (first
                                       escalation step for ill-conditioned systems) */
@@ -106,6 +115,9 @@ typedef struct {
                                       the residual is <= rtol and the error estimated
                                       from the last two corrections is <= xtol
                                       (default 1e-8) */
+    int refactor_threads;          /* CTA size of the refactorization kernel: 0 auto
+                                      (1024 when the batch has at most one system per
+                                      SM, else 256), or 64..1024, a multiple of 32 */
 } lusp_batch_opts;
 
 /* ---- library ---- */
@@ -119,6 +131,12 @@ int lusp_device_count(void);
  * and lusp_last_error names the column. */
 int lusp_pattern_create(int n, const int *Ap, const int *Ai, const double *Ax,
                         const int *q, lusp_pattern **out);
+/* As lusp_pattern_create, with the size of the dense trailing block: the
+ * last dense_tail columns (and rows) are refactored and solved as one dense
+ * block (at most 768; -1: chosen by a cost model, which lusp_pattern_create
+ * uses; 0: none).  The factor values are the same either way. */
+int lusp_pattern_create_ex(int n, const int *Ap, const int *Ai, const double *Ax,
+                           const int *q, int dense_tail, lusp_pattern **out);
 void lusp_pattern_destroy(lusp_pattern *p);
 int lusp_pattern_get_info(const lusp_pattern *p, lusp_pattern_info *info);
 /* pinv[orig_row] = position; q[position] = original column. */

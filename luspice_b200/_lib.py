@@ -20,7 +20,8 @@ class PatternInfo(C.Structure):
                 ("cap", C.c_long), ("ncol_levels", C.c_int), ("nfwd_levels", C.c_int),
                 ("nbwd_levels", C.c_int), ("max_col", C.c_int), ("nslices", C.c_int),
                 ("sell_total", C.c_int), ("flops", C.c_long), ("gathered", C.c_long),
-                ("hash", C.c_ulonglong), ("device_bytes", C.c_size_t), ("singular_col", C.c_int)]
+                ("hash", C.c_ulonglong), ("device_bytes", C.c_size_t), ("singular_col", C.c_int),
+                ("dense_tail", C.c_int), ("tail_start", C.c_int)]
 
 
 class SysStats(C.Structure):
@@ -28,7 +29,10 @@ class SysStats(C.Structure):
                 ("max_abs_u", C.c_double), ("res", C.c_double * 16), ("nres", C.c_int),
                 ("inner_iters", C.c_int), ("outer_iters", C.c_int), ("status", C.c_int),
                 ("singular_col", C.c_int), ("pad_", C.c_int), ("cyc_wait", C.c_longlong),
-                ("cyc_gather", C.c_longlong), ("cyc_update", C.c_longlong), ("cyc_refactor", C.c_longlong)]
+                ("cyc_gather", C.c_longlong), ("cyc_update", C.c_longlong), ("cyc_refactor", C.c_longlong),
+                ("cyc_lsolve", C.c_longlong), ("cyc_tail", C.c_longlong), ("cyc_usolve", C.c_longlong),
+                ("cyc_spmv", C.c_longlong), ("cyc_solve", C.c_longlong), ("cyc_tpanel", C.c_longlong),
+                ("cyc_ttrsm", C.c_longlong), ("cyc_tupdate", C.c_longlong)]
 
 
 class BatchOpts(C.Structure):
@@ -36,7 +40,7 @@ class BatchOpts(C.Structure):
                 ("rtol", C.c_double), ("inner_rel", C.c_double), ("stag_ratio", C.c_double),
                 ("pivot_tol", C.c_double), ("block_threads", C.c_int), ("ctas_per_sm", C.c_int),
                 ("solve_sweep", C.c_int), ("refactor_mode", C.c_int), ("inner_prec", C.c_int),
-                ("xtol", C.c_double)]
+                ("xtol", C.c_double), ("refactor_threads", C.c_int)]
 
 
 class ServerOpts(C.Structure):
@@ -94,6 +98,7 @@ SIGNATURES = {
     "lusp_version": (C.c_char_p, []),
     "lusp_device_count": (C.c_int, []),
     "lusp_pattern_create": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, c_void_pp]),
+    "lusp_pattern_create_ex": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, C.c_int, c_void_pp]),
     "lusp_pattern_destroy": (None, [C.c_void_p]),
     "lusp_pattern_get_info": (C.c_int, [C.c_void_p, C.POINTER(PatternInfo)]),
     "lusp_pattern_get_perm": (C.c_int, [C.c_void_p, c_int_p, c_int_p]),

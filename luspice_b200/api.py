@@ -53,14 +53,17 @@ def _stream(s) -> C.c_void_p:
 class Pattern:
     """Host analysis + device-resident static layout of one sparsity pattern."""
 
-    def __init__(self, n: int, Ap, Ai, Ax, q=None):
+    def __init__(self, n: int, Ap, Ai, Ax, q=None, dense_tail: int = -1):
+        """dense_tail: trailing columns factored and solved as one dense
+        block (-1 chosen by the library's cost model, 0 none)."""
         lib = L.load()
         self.n = int(n)
         self._Ap, self._Ai, self._Ax = _i32(Ap), _i32(Ai), _f64(Ax)
         qq = None if q is None else _i32(q)
         h = C.c_void_p()
-        rc = lib.lusp_pattern_create(self.n, L.ptr(self._Ap, C.c_int), L.ptr(self._Ai, C.c_int),
-                                     L.ptr(self._Ax, C.c_double), L.ptr(qq, C.c_int), C.byref(h))
+        rc = lib.lusp_pattern_create_ex(self.n, L.ptr(self._Ap, C.c_int), L.ptr(self._Ai, C.c_int),
+                                        L.ptr(self._Ax, C.c_double), L.ptr(qq, C.c_int), int(dense_tail),
+                                        C.byref(h))
         _check(rc, "lusp_pattern_create")
         self.handle = h
         info = L.PatternInfo()
@@ -68,8 +71,8 @@ class Pattern:
         self.info = {k: getattr(info, k) for k, _ in L.PatternInfo._fields_}
 
     @classmethod
-    def from_matrix(cls, m, q=None, values=None):
-        return cls(m.n, m.Ap, m.Ai, m.Ax if values is None else values, q)
+    def from_matrix(cls, m, q=None, values=None, dense_tail: int = -1):
+        return cls(m.n, m.Ap, m.Ai, m.Ax if values is None else values, q, dense_tail)
 
     def perm(self) -> tuple[np.ndarray, np.ndarray]:
         pinv = np.empty(self.n, np.int32)

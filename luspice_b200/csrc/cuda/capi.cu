@@ -38,11 +38,17 @@ int lusp_device_count(void) {
 
 int lusp_pattern_create(int n, const int* Ap, const int* Ai, const double* Ax, const int* q,
                         lusp_pattern** out) {
+    return lusp_pattern_create_ex(n, Ap, Ai, Ax, q, -1, out);
+}
+
+int lusp_pattern_create_ex(int n, const int* Ap, const int* Ai, const double* Ax, const int* q,
+                           int dense_tail, lusp_pattern** out) {
     if (!out) return LUSP_EARG;
     *out = nullptr;
+    if (dense_tail < -1) { lusp::set_error("pattern_create: dense_tail must be >= -1"); return LUSP_EARG; }
     try {
         PatternObj* P = nullptr;
-        int rc = lusp::pattern_build(n, Ap, Ai, Ax, q, &P);
+        int rc = lusp::pattern_build(n, Ap, Ai, Ax, q, &P, dense_tail);
         if (rc == LUSP_OK) *out = reinterpret_cast<lusp_pattern*>(P);
         return rc;
     } catch (const std::bad_alloc&) {
@@ -73,6 +79,8 @@ int lusp_pattern_get_info(const lusp_pattern* hp, lusp_pattern_info* info) {
     info->hash = S.hash;
     info->device_bytes = PO(hp)->bytes;
     info->singular_col = -1;
+    info->dense_tail = S.dtail;
+    info->tail_start = S.k0;
     return LUSP_OK;
 }
 
@@ -152,6 +160,7 @@ void lusp_batch_opts_default(lusp_batch_opts* o) {
     o->refactor_mode = 0;
     o->inner_prec = 0;
     o->xtol = 1e-8;
+    o->refactor_threads = 0;
 }
 
 int lusp_batch_create(int nsys, lusp_pattern* const* pats, const lusp_batch_opts* opts,
@@ -237,7 +246,7 @@ int lusp_batch_run_graph(lusp_batch* hb, int what, void* stream) {
     }
     cudaError_t e = cudaGraphLaunch(it->second.exec, st);
     if (e != cudaSuccess) return lusp::cuda_fail(e, "graph launch");
-    B->launches = 1;
+    B->launches = lusp::launch_kernel_count(what);
     return LUSP_OK;
 }
 

@@ -44,13 +44,15 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 // ---------------------------------------------------------------------------
-// The persistent kernel: every CTA takes systems from the device work queue
-// until it is empty; for each one it runs the requested phases.
+// The persistent kernels: every CTA takes systems from a device work queue
+// until it is empty.  The refactorization runs as its own kernel (many warps
+// per CTA, few registers each); the solve kernel runs the triangular solves
+// and GMRES-IR (fewer warps, more registers).  queue[0] feeds the refactor
+// kernel, queue[1] the solve kernel.
 // ---------------------------------------------------------------------------
-template <typename VT, typename AT>
-__global__ void __launch_bounds__(512)
-batch_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan,
-             SolveParams prm, int what, int direct) {
+template <typename VT>
+__global__ void __launch_bounds__(1024, 1)
+refactor_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan, SolveParams prm) {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_task;
     while (true) {
@@ -60,11 +62,35 @@ batch_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan
         const int t = s_task;
         if (t >= nsys) break;
         const SysDev S = sys[t];
-        if (what & LUSP_RUN_REFACTOR) refactor_phase<VT>(S, plan, smem, prm);
-        if (what & LUSP_RUN_SOLVE) {
-            if (direct) direct_phase<VT>(S, plan, smem);
-            else gmres_phase<VT, AT>(S, plan, smem, prm);
+        refactor_phase<VT>(S, plan, smem, prm);
+    }
+}
+
+template <typename VT, typename AT>
+__global__ void __launch_bounds__(512)
+solve_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan,
+             SolveParams prm, int direct) {
+    extern __shared__ __align__(16) char smem[];
+    __shared__ int s_task;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_task = atomicAdd(queue + 1, 1);
+        __syncthreads();
+        const int t = s_task;
+        if (t >= nsys) break;
+        const SysDev S = sys[t];
+        const long long ts = clock64();
+        if (threadIdx.x == 0) {
+            S.stats->cyc_lsolve = 0;
+            S.stats->cyc_tail = 0;
+            S.stats->cyc_usolve = 0;
+            S.stats->cyc_spmv = 0;
         }
+        __syncthreads();
+        if (direct) direct_phase<VT>(S, plan, smem);
+        else gmres_phase<VT, AT>(S, plan, smem, prm);
+        __syncthreads();
+        if (threadIdx.x == 0) S.stats->cyc_solve = clock64() - ts;
     }
 }
 
@@ -80,7 +106,7 @@ static int upload_ints(const std::vector<int>& v, int* dst, cudaStream_t) {
 }
 
 int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const int* q_in,
-                  PatternObj** out) {
+                  PatternObj** out, int dense_tail) {
     *out = nullptr;
     if (n <= 0 || !Ap || !Ai || !Ax) { set_error("pattern_create: bad arguments"); return LUSP_EARG; }
     const int nnz = Ap[n];
@@ -129,7 +155,7 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
         return LUSP_ESINGULAR;
     }
     PatternObj* P = new PatternObj();
-    build_static_pattern(n, Ap, Ai, q.data(), F, 256, P->S);
+    build_static_pattern(n, Ap, Ai, q.data(), F, 256, P->S, dense_tail);
     const StaticPattern& S = P->S;
 
     // One device block for every int array of the layout.
@@ -183,6 +209,28 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     D.bwd_lev = blk + off[idx++];
     D.nfwd_levels = S.nfwd_levels;
     D.nbwd_levels = S.nbwd_levels;
+    D.k0 = S.k0;
+    D.dtail = S.dtail;
+    D.tail_ld = tail_ld(S);
+    // Relative update slots: rel_ptr (n+1 int64) then rel (16 bit, padded by
+    // 16 entries so aligned 16-byte copies never run past the end).
+    D.rel = nullptr;
+    D.rel_ptr = nullptr;
+    if (!S.rel_ptr.empty()) {
+        const size_t pbytes = ((S.rel_ptr.size() * sizeof(long long)) + 255) & ~(size_t)255;
+        const size_t rbytes = (S.rel.size() + 16) * sizeof(uint16_t);
+        e = cudaMalloc(&P->d_rel, pbytes + rbytes);
+        if (e != cudaSuccess) { pattern_free(P); return cuda_fail(e, "pattern rel alloc"); }
+        char* rb = (char*)P->d_rel;
+        e = cudaMemcpy(rb, S.rel_ptr.data(), S.rel_ptr.size() * sizeof(long long), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !S.rel.empty())
+            e = cudaMemcpy(rb + pbytes, S.rel.data(), S.rel.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(rb + pbytes + S.rel.size() * sizeof(uint16_t), 0, 16 * sizeof(uint16_t));
+        if (e != cudaSuccess) { pattern_free(P); return cuda_fail(e, "pattern rel upload"); }
+        D.rel_ptr = (const long long*)rb;
+        D.rel = (const unsigned short*)(rb + pbytes);
+        P->bytes += pbytes + rbytes;
+    }
     e = cudaMalloc(&P->d_desc, sizeof(PatternDev));
     if (e != cudaSuccess) { pattern_free(P); return cuda_fail(e, "pattern descriptor alloc"); }
     e = cudaMemcpy(P->d_desc, &D, sizeof(PatternDev), cudaMemcpyHostToDevice);
@@ -194,6 +242,7 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
 void pattern_free(PatternObj* P) {
     if (!P) return;
     if (P->d_block) cudaFree(P->d_block);
+    if (P->d_rel) cudaFree(P->d_rel);
     if (P->d_desc) cudaFree(P->d_desc);
     delete P;
 }
@@ -215,20 +264,22 @@ static size_t smem_fixed(int nwords) { return 64 + (((size_t)nwords * 4 + 15) & 
 
 void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm, int m, int vsize,
                SmemPlan& plan) {
-    int nmax = 1, colmax = 1, levmax = 1;
+    (void)vsize;
+    int nmax = 1, levmax = 1;
     for (auto* p : pats) {
         nmax = std::max(nmax, p->S.n);
-        colmax = std::max(colmax, p->S.max_col);
         levmax = std::max(levmax, p->S.nfwd_levels + p->S.nbwd_levels);
     }
+    (void)block;
     const size_t limit = 227 * 1024;
     size_t budget = 228 * 1024 / std::max(1, ctas_per_sm);
     budget = budget > 1024 ? budget - 1024 : budget;
     budget = std::min(budget, limit);
     plan.nwords = (nmax + 31) / 32;
     plan.m = m;
+    plan.wcap = 0;
+    plan.scap = 0;
     const size_t fixed = smem_fixed(plan.nwords);
-    const int nw = block / 32;
     const size_t hbytes = ((size_t)(m + 1) * m + 6 * (size_t)(m + 1)) * sizeof(double);
     size_t avail = budget > fixed + hbytes ? budget - fixed - hbytes : 0;
     // Solve vector in shared memory when it fits, and the level-sweep
@@ -237,46 +288,98 @@ void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm,
     plan.ycap = ((size_t)nmax * 8 <= avail) ? nmax : 0;
     const size_t dneed = 4 * (size_t)nmax + (size_t)levmax + 8;
     plan.dcap = (plan.ycap && (size_t)nmax * 8 + dneed * 4 <= avail) ? (int)dneed : 0;
-    // Refactor area per warp: the work vector and rows of one column (up to
-    // the longest column; longer ones spill to global scratch) plus a stage
-    // of 512 gathered L entries (at least 64).
-    const size_t per_warp = budget > fixed ? (budget - fixed) / nw : 0;
-    const size_t stage_entry = 4 + (size_t)vsize;
-    int scap = 512;
-    while (scap > 64 && (size_t)scap * stage_entry > per_warp / 2) scap /= 2;
-    size_t left = per_warp > (size_t)scap * stage_entry ? per_warp - (size_t)scap * stage_entry : 0;
-    plan.wcap = (int)std::min<size_t>((size_t)colmax, left / 12);
-    plan.scap = scap;
-    // Row -> slot map (16-bit slots, n entries per warp) when it fits in what
-    // is left: replaces a binary search per gathered entry by one lookup.
-    left = left > (size_t)plan.wcap * 12 ? left - (size_t)plan.wcap * 12 : 0;
-    const size_t mneed = (((size_t)nmax * 2 + 15) & ~(size_t)15) / 2;
-    plan.mcap = (nmax <= 65535 && colmax <= 65535 && mneed * 2 <= left) ? (int)mneed : 0;
-    const size_t solve_bytes = (size_t)plan.ycap * 8 + hbytes + (size_t)plan.dcap * 4;
-    const size_t ref_bytes = (size_t)nw * ((size_t)plan.wcap * 12 + (size_t)plan.scap * stage_entry +
-                                           (size_t)plan.mcap * 2);
-    plan.bytes = fixed + std::max(solve_bytes, ref_bytes);
+    plan.bytes = fixed + (size_t)plan.ycap * 8 + hbytes + (size_t)plan.dcap * 4;
 }
 
-// Raise the dynamic shared-memory limit of one kernel instantiation (once
-// per size; not a stream operation, so it stays out of captured graphs after
-// the first call) and optionally report its occupancy.
-template <typename VT, typename AT>
-static int kernel_prepare(size_t smem, int block, int* occ) {
-    auto kern = batch_kernel<VT, AT>;
-    static std::mutex mu;
-    static size_t granted = 0;
+int refactor_block(const lusp_batch_opts& o, int nsys) {
+    if (o.refactor_threads > 0) return o.refactor_threads;
+    return nsys <= sm_count() ? 1024 : 256;
+}
+
+void make_refactor_plan(const std::vector<PatternObj*>& pats, int threads, int vsize, SmemPlan& plan) {
+    int nmax = 1, colmax = 2;
+    for (auto* p : pats) {
+        nmax = std::max(nmax, p->S.n);
+        colmax = std::max(colmax, p->S.max_col);
+    }
+    colmax = (colmax + 1) & ~1;
+    // Target 32 resident warps per SM: one 1024-thread CTA, or several
+    // smaller ones.
+    const int ctas = std::max(1, 1024 / threads);
+    size_t budget = std::min<size_t>(227 * 1024, 228 * 1024 / ctas - 1024);
+    plan.nwords = (nmax + 31) / 32;
+    plan.m = 0;
+    plan.ycap = 0;
+    plan.dcap = 0;
+    const size_t fixed = smem_fixed(plan.nwords);
+    const int nw = threads / 32;
+    const size_t per_warp = budget > fixed ? (budget - fixed) / nw : 0;
+    // Per warp: work vector (wcap fp64), stage of scap values and scap + 16
+    // relative slots.  Prefer the whole longest column in shared memory,
+    // then the largest stage (512 down to 64 entries).
+    auto need = [&](int wcap, int scap) {
+        return (size_t)wcap * 8 + (size_t)scap * vsize + ((size_t)scap + 16) * 2;
+    };
+    int scap = 512;
+    while (scap > 64 && need(colmax, scap) > per_warp) scap /= 2;
+    int wcap = colmax;
+    if (need(wcap, scap) > per_warp) {
+        const size_t rest = per_warp > need(0, scap) ? per_warp - need(0, scap) : 0;
+        wcap = (int)std::min<size_t>((size_t)colmax, rest / 8) & ~1;
+    }
+    plan.wcap = wcap;
+    plan.scap = scap;
+    plan.bytes = fixed + (size_t)nw * need(wcap, scap);
+    // Dense trailing block: panel [D][nb] + U tile [nb][64] + nb column
+    // maxima, reusing the per-warp area after the sparse phase.  Widest
+    // panel (32, 16, 8) that fits the budget.
+    int dmax = 0;
+    for (auto* p : pats) dmax = std::max(dmax, p->S.dtail);
+    plan.tnb = 0;
+    if (dmax > 0) {
+        auto dneed = [&](int nb) { return fixed + 8 * ((size_t)dmax * nb + (size_t)nb * 64 + nb); };
+        int nb = 32;
+        while (nb > 8 && dneed(nb) > std::max(budget, plan.bytes)) nb /= 2;
+        plan.tnb = nb;
+        plan.bytes = std::max(plan.bytes, dneed(nb));
+    }
+}
+
+// Raise the dynamic shared-memory limit of one kernel (once per size; not a
+// stream operation, so it stays out of captured graphs after the first
+// call) and optionally report its occupancy.
+template <typename K>
+static int prepare_kernel(K kern, size_t smem, int block, int* occ, size_t* granted, std::mutex& mu) {
     std::lock_guard<std::mutex> lk(mu);
-    if (smem > granted) {
+    if (smem > *granted) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return cuda_fail(e, "kernel smem attribute");
-        granted = smem;
+        *granted = smem;
     }
     if (occ) {
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, block, smem);
         if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
     }
     return LUSP_OK;
+}
+
+template <typename VT, typename AT>
+static int kernel_prepare(size_t smem, int block, int* occ) {
+    static std::mutex mu;
+    static size_t granted = 0;
+    return prepare_kernel(solve_kernel<VT, AT>, smem, block, occ, &granted, mu);
+}
+
+template <typename VT>
+static int refactor_prepare(size_t smem, int block, int* occ) {
+    static std::mutex mu;
+    static size_t granted = 0;
+    return prepare_kernel(refactor_kernel<VT>, smem, block, occ, &granted, mu);
+}
+
+int refactor_occupancy(int prec, size_t smem, int block, int* occ) {
+    if (prec == LUSP_FP64) return refactor_prepare<double>(smem, block, occ);
+    return refactor_prepare<float>(smem, block, occ);
 }
 
 int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ) {
@@ -287,15 +390,24 @@ int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ) {
 
 template <typename VT, typename AT>
 static int launch_typed(const LaunchArgs& a, cudaStream_t st) {
-    int rc = kernel_prepare<VT, AT>(a.plan.bytes, a.block, nullptr);
-    if (rc != LUSP_OK) return rc;
-    cudaError_t e = cudaMemsetAsync(a.d_queue, 0, sizeof(int), st);
+    cudaError_t e = cudaMemsetAsync(a.d_queue, 0, 2 * sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "queue reset");
-    const int direct = (a.prec == LUSP_FP64 || (a.what & LUSP_RUN_DIRECT)) ? 1 : 0;
-    batch_kernel<VT, AT><<<a.grid, a.block, a.plan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.plan, a.prm,
-                                                              a.what & 3, direct);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "batch kernel launch");
+    if (a.what & LUSP_RUN_REFACTOR) {
+        int rc = refactor_prepare<VT>(a.rplan.bytes, a.rblock, nullptr);
+        if (rc != LUSP_OK) return rc;
+        refactor_kernel<VT><<<a.rgrid, a.rblock, a.rplan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.rplan, a.prm);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "refactor kernel launch");
+    }
+    if (a.what & LUSP_RUN_SOLVE) {
+        int rc = kernel_prepare<VT, AT>(a.plan.bytes, a.block, nullptr);
+        if (rc != LUSP_OK) return rc;
+        const int direct = (a.prec == LUSP_FP64 || (a.what & LUSP_RUN_DIRECT)) ? 1 : 0;
+        solve_kernel<VT, AT><<<a.grid, a.block, a.plan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.plan, a.prm,
+                                                                  direct);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "solve kernel launch");
+    }
     return LUSP_OK;
 }
 
@@ -305,26 +417,40 @@ int launch_systems(const LaunchArgs& a, cudaStream_t st) {
     return launch_typed<float, float>(a, st);
 }
 
+int launch_kernel_count(int what) {
+    return ((what & LUSP_RUN_REFACTOR) ? 1 : 0) + ((what & LUSP_RUN_SOLVE) ? 1 : 0);
+}
+
 int batch_launch(BatchObj* B, int what, cudaStream_t st) {
     LaunchArgs a = B->launch;
     a.what = what;
     int rc = launch_systems(a, st);
-    if (rc == LUSP_OK) B->launches = 1;
+    if (rc == LUSP_OK) B->launches = launch_kernel_count(what);
     return rc;
 }
 
 static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+int tail_ld(const StaticPattern& S) { return (S.dtail + 31) & ~31; }
+
 size_t system_private_bytes(const StaticPattern& S, size_t vs, int m) {
     const size_t n = S.n;
     const size_t st = S.sell_ptr.back();
     return al256(S.cap * vs) + al256(S.lci.size() * vs) + al256(S.uci.size() * vs) + al256(n * vs) +
-           al256(st * 8) + al256(st * 4) + al256(((size_t)m + 8) * n * 8);
+           al256(st * 8) + al256(st * 4) + al256(((size_t)m + 8) * n * 8) +
+           al256((size_t)S.dtail * tail_ld(S) * vs);
+}
+
+size_t tail_work_doubles(const std::vector<PatternObj*>& pats) {
+    size_t m = 0;
+    for (auto* p : pats) m = std::max(m, (size_t)p->S.dtail * tail_ld(p->S));
+    return (m + 31) & ~(size_t)31;
 }
 
 char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m) {
     const size_t n = S.n;
     const size_t st = S.sell_ptr.back();
+    D.tail = p; p += al256((size_t)S.dtail * tail_ld(S) * vs);
     D.lu = p; p += al256(S.cap * vs);
     D.lval = p; p += al256(S.lci.size() * vs);
     D.uval = p; p += al256(S.uci.size() * vs);
@@ -335,8 +461,8 @@ char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m)
     return p;
 }
 
-size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& plan) {
-    return colmax > plan.wcap ? al256((size_t)grid * (block / 32) * colmax * 8) : 0;
+size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& rplan) {
+    return colmax > rplan.wcap ? al256((size_t)grid * (block / 32) * colmax * 8) : 0;
 }
 
 int check_opts(const lusp_batch_opts* o) {
@@ -344,6 +470,11 @@ int check_opts(const lusp_batch_opts* o) {
     if (o->krylov < 1 || o->krylov > kMaxKrylov) { set_error("krylov must be 1..%d", kMaxKrylov); return LUSP_EARG; }
     if (o->block_threads < 64 || o->block_threads > 512 || o->block_threads % 32) { set_error("block_threads must be 64..512, a multiple of 32"); return LUSP_EARG; }
     if (o->inner_prec < 0 || o->inner_prec > 1) { set_error("bad inner_prec"); return LUSP_EARG; }
+    if (o->refactor_threads != 0 &&
+        (o->refactor_threads < 64 || o->refactor_threads > 1024 || o->refactor_threads % 32)) {
+        set_error("refactor_threads must be 0 (auto) or 64..1024, a multiple of 32");
+        return LUSP_EARG;
+    }
     return LUSP_OK;
 }
 
@@ -356,6 +487,17 @@ void fill_params(SolveParams& prm, const lusp_batch_opts& o) {
     prm.pivot_tol = o.pivot_tol;
     prm.refactor_mode = o.refactor_mode;
     prm.xtol = o.xtol > 0 ? o.xtol : 1e-8;
+}
+
+int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, int nsys, LaunchArgs& a) {
+    a.rblock = refactor_block(o, nsys);
+    make_refactor_plan(pats, a.rblock, o.prec == LUSP_FP64 ? 8 : 4, a.rplan);
+    int occ = 0;
+    int rc = refactor_occupancy(o.prec, a.rplan.bytes, a.rblock, &occ);
+    if (rc != LUSP_OK) return rc;
+    if (occ < 1) { set_error("refactor kernel does not fit one SM (smem %zu)", a.rplan.bytes); return LUSP_EARG; }
+    a.rgrid = std::min(nsys, occ * sm_count());
+    return LUSP_OK;
 }
 
 int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, SmemPlan& plan) {
@@ -404,8 +546,14 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     if (rc != LUSP_OK) { delete B; return rc; }
     if (occ < 1) { delete B; set_error("batch_create: kernel does not fit one SM (smem %zu)", B->plan.bytes); return LUSP_EARG; }
     B->grid = std::min(nsys, occ * sm_count());
-    const size_t spill = spill_bytes(B->grid, B->block, colmax, B->plan);
-    const size_t total = base[nsys] + spill + al256(sizeof(SysStats) * nsys) + al256(sizeof(SysDev) * nsys) + 256;
+    LaunchArgs& a = B->launch;
+    rc = refactor_setup(B->pats, *o, nsys, a);
+    if (rc != LUSP_OK) { delete B; return rc; }
+    const size_t spill = spill_bytes(a.rgrid, a.rblock, colmax, a.rplan);
+    const size_t tws = tail_work_doubles(B->pats);
+    const size_t tail_bytes = al256((size_t)a.rgrid * tws * 8);
+    const size_t total = base[nsys] + spill + tail_bytes + al256(sizeof(SysStats) * nsys) +
+                         al256(sizeof(SysDev) * nsys) + 256;
     char* blk = nullptr;
     cudaError_t e = cudaMalloc(&blk, total);
     if (e != cudaSuccess) { delete B; return cuda_fail(e, "batch device alloc"); }
@@ -413,7 +561,8 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     B->bytes = total;
     e = cudaMemset(blk, 0, total);
     if (e != cudaSuccess) { batch_free(B); return cuda_fail(e, "batch memset"); }
-    char* stats_base = blk + base[nsys] + spill;
+    double* tail_ptr = tws ? (double*)(blk + base[nsys] + spill) : nullptr;
+    char* stats_base = blk + base[nsys] + spill + tail_bytes;
     B->d_stats = (SysStats*)stats_base;
     B->d_sys = (SysDev*)(stats_base + al256(sizeof(SysStats) * nsys));
     B->d_queue = (int*)((char*)B->d_sys + al256(sizeof(SysDev) * nsys));
@@ -430,11 +579,12 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
         D.x = B->d_x + B->vec_off[s];
         carve_system(D, blk + base[s], B->pats[s]->S, vs, o->krylov);
         D.scratch = spill_ptr;
+        D.tailws = tail_ptr;
+        D.tailws_stride = (long long)tws;
         D.stats = B->d_stats + s;
     }
     e = cudaMemcpy(B->d_sys, B->h_sys.data(), sizeof(SysDev) * nsys, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { batch_free(B); return cuda_fail(e, "batch descriptor upload"); }
-    LaunchArgs& a = B->launch;
     a.d_sys = B->d_sys;
     a.nsys = nsys;
     a.d_queue = B->d_queue;

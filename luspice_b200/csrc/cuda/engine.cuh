@@ -41,6 +41,11 @@ struct PatternDev {
     const int* sell_perm;    // [32*nslices] row position or -1
     const int* rowat;        // [n] position -> original row
     const int* q;            // [n] position -> original column
+    const unsigned short* rel;    // relative update slots (null: search rows)
+    const long long* rel_ptr;     // [n+1] column k's list in rel
+    // Dense trailing block: rows/columns [k0, n), dtail = n - k0 (0: none),
+    // stored row-major with leading dimension tail_ld.
+    int k0, dtail, tail_ld;
 };
 
 // Per-system statistics written by the kernels.
@@ -58,6 +63,11 @@ struct SysStats {
     // SM cycles (summed over warps): refactor waits for dependency columns,
     // gathers of their L parts, updates; refactor wall cycles of the CTA.
     long long cyc_wait, cyc_gather, cyc_update, cyc_refactor;
+    // SM cycles of the solve (CTA wall time, summed over calls): L sweeps,
+    // dense-tail solves, U sweeps, SpMVs, whole solve phase.
+    long long cyc_lsolve, cyc_tail, cyc_usolve, cyc_spmv, cyc_solve;
+    // Refactor: dense trailing block panels, U-row solves, trailing updates.
+    long long cyc_tpanel, cyc_ttrsm, cyc_tupdate;
 };
 
 // One system: pattern + values + vectors + workspace.
@@ -75,6 +85,10 @@ struct SysDev {
     double* work;            // workspace (see solve phase)
     double* scratch;         // per-CTA refactor spill (columns longer than
                              // the shared-memory work area), may be null
+    void* tail;              // [dtail * tail_ld] dense L\U of the trailing
+                             // block (VT), unit L below the diagonal
+    double* tailws;          // refactor CTAs' fp64 trailing-block work areas
+    long long tailws_stride; // doubles per CTA in tailws
     SysStats* stats;
 };
 
@@ -96,7 +110,7 @@ struct SmemPlan {
     int nwords;              // ready-bit words (>= ceil(n_max/32))
     int wcap;                // per-warp refactor work slots
     int scap;                // per-warp staged L entries (refactor gathers)
-    int mcap;                // per-warp row -> slot map entries (0 = none)
+    int tnb;                 // panel width of the dense trailing block
     int ycap;                // doubles for a shared-memory solve vector
     int dcap;                // ints for shared-memory sweep descriptors
     int m;                   // Krylov dimension for H

@@ -18,6 +18,7 @@ struct PatternObj {
     PatternDev desc{};               // host copy holding device pointers
     PatternDev* d_desc = nullptr;
     int* d_block = nullptr;
+    void* d_rel = nullptr;           // relative update slots (rel_ptr, rel)
     size_t bytes = 0;
 };
 
@@ -34,6 +35,9 @@ struct LaunchArgs {
     int what = LUSP_RUN_BOTH;
     int block = 256;
     int grid = 1;
+    SmemPlan rplan{};                // refactorization kernel
+    int rblock = 1024;
+    int rgrid = 1;
 };
 
 struct GraphEntry {
@@ -68,8 +72,9 @@ struct BatchObj {
 void set_error(const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);
 
+// dense_tail: -1 cost model, 0 none, > 0 that many trailing columns.
 int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const int* q,
-                  PatternObj** out);
+                  PatternObj** out, int dense_tail = -1);
 void pattern_free(PatternObj* P);
 
 void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm, int m, int vsize,
@@ -81,9 +86,19 @@ int check_opts(const lusp_batch_opts* o);
 void fill_params(SolveParams& prm, const lusp_batch_opts& o);
 int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, SmemPlan& plan);
 int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ);
+int refactor_occupancy(int prec, size_t smem, int block, int* occ);
+int refactor_block(const lusp_batch_opts& o, int nsys);
+void make_refactor_plan(const std::vector<PatternObj*>& pats, int threads, int vsize, SmemPlan& plan);
+// Refactorization kernel block, plan and grid for nsys systems of pats.
+int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, int nsys, LaunchArgs& a);
+// Kernels one launch with these RUN_* flags issues.
+int launch_kernel_count(int what);
 size_t system_private_bytes(const StaticPattern& S, size_t vs, int m);
+int tail_ld(const StaticPattern& S);
+// fp64 trailing-block work area of one refactor CTA (doubles).
+size_t tail_work_doubles(const std::vector<PatternObj*>& pats);
 char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m);
-size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& plan);
+size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& rplan);
 int launch_systems(const LaunchArgs& a, cudaStream_t st);
 int sm_count();
 void batch_free(BatchObj* B);

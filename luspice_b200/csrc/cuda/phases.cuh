@@ -36,12 +36,6 @@ __device__ __forceinline__ int find_slot(const int* rows, int lo, int hi, int i)
     return (lo < end && rows[lo] == i) ? lo : -1;
 }
 
-// Slot of row i through the column's row -> slot map, or -1.
-__device__ __forceinline__ int map_slot(const unsigned short* map, const int* rows, int len, int i) {
-    const int s = map[i];
-    return (s < len && rows[s] == i) ? s : -1;
-}
-
 // Non-blocking test of a ready bit.
 __device__ __forceinline__ bool is_ready(const unsigned* bits, int j) {
     return (*((const volatile unsigned*)bits + (j >> 5)) >> (j & 31)) & 1u;
@@ -68,18 +62,243 @@ __device__ __forceinline__ int warp_claim(int* counter) {
 }
 
 // ---------------------------------------------------------------------------
+// Dense trailing block of the refactorization (rows and columns [k0, n)),
+// in place in W (fp64, row-major, leading dimension ld).  On entry W holds
+// the block after the updates from the columns before k0; on exit its strict
+// lower part holds the stored (VT-rounded) multipliers and its upper part
+// the fp64 U values.  Right-looking with panels of nb columns (the panel in
+// shared memory): entry (i, c) still receives its updates in ascending order
+// of the pivot column, each a separately rounded multiply and subtract with
+// the stored multiplier and the fp64 U value, so the factor equals the
+// column engine's bit for bit.  Pivot statistics as in the column engine.
+// ---------------------------------------------------------------------------
+template <typename VT>
+__device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, const SmemPlan& plan,
+                                  const SolveParams& prm, double& minpiv, double& minratio, int& bad,
+                                  SysStats* st) {
+    long long c_pan = 0, c_trsm = 0, c_upd = 0, tk = clock64();
+    const int D = P.dtail, ld = P.tail_ld, k0 = P.k0, nb = plan.tnb;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+    double* pan = (double*)sm.uni;                                           // [D][nb]
+    double* ut = pan + (size_t)D * nb;                                       // [nb][64]
+    unsigned long long* cmax = (unsigned long long*)(ut + (size_t)nb * 64);  // [nb]
+    const int tx = tid & 63, ty = tid >> 6, nty = nt >> 6;
+    for (int jb = 0; jb < D; jb += nb) {
+        const int w = min(nb, D - jb), R = D - jb;
+        for (int t = tid; t < R * nb; t += nt) {
+            const int r = t / nb, c = t - r * nb;
+            pan[t] = c < w ? W[(size_t)(jb + r) * ld + jb + c] : 0.0;
+        }
+        if (tid < nb) cmax[tid] = 0ull;
+        __syncthreads();
+        // Panel: unblocked elimination.  Per column: the multipliers (one
+        // thread per row, all divisions in flight together), then the update
+        // of the columns to the right (a warp per row, lanes = columns).
+        const int warp = tid >> 5, nw = nt >> 5;
+        for (int c = 0; c < w; c++) {
+            const double piv = pan[c * nb + c];
+            double lm = 0.0;
+            for (int r = c + 1 + tid; r < R; r += nt) {
+                const double v = pan[r * nb + c];
+                lm = fmax(lm, fabs(v));
+                pan[r * nb + c] = (double)ValTraits<VT>::to(__ddiv_rn(v, piv));
+            }
+            lm = warp_max(lm);
+            if (lane == 0 && lm > 0.0) atomicMax(&cmax[c], (unsigned long long)__double_as_longlong(lm));
+            __syncthreads();
+            if (c + 1 < w) {
+                const double uc = lane < w ? pan[c * nb + lane] : 0.0;
+                const bool act = lane > c && lane < w;
+                int r = c + 1 + warp;
+                for (; r + nw < R; r += 2 * nw) {
+                    double* r0 = pan + (size_t)r * nb;
+                    double* r1 = r0 + (size_t)nw * nb;
+                    const double l0 = r0[c], l1 = r1[c];
+                    if (act) {
+                        const double a0 = r0[lane], a1 = r1[lane];
+                        r0[lane] = __dsub_rn(a0, __dmul_rn(l0, uc));
+                        r1[lane] = __dsub_rn(a1, __dmul_rn(l1, uc));
+                    }
+                }
+                if (r < R && act) {
+                    double* r0 = pan + (size_t)r * nb;
+                    r0[lane] = __dsub_rn(r0[lane], __dmul_rn(r0[c], uc));
+                }
+                __syncthreads();
+            }
+        }
+        if (tid < w) {
+            const int c = tid;
+            const double piv = pan[c * nb + c];
+            const double ap = fabs(piv);
+            const double amax = __longlong_as_double((long long)cmax[c]);
+            if (!(ap > 0.0) || !isfinite(piv)) {
+                bad |= ST_SINGULAR;
+                atomicMin(&sm.ctl[2], k0 + jb + c);
+            }
+            minpiv = fmin(minpiv, ap);
+            const double ratio = amax > ap ? ap / amax : 1.0;
+            minratio = fmin(minratio, ratio);
+            if (ratio < prm.pivot_tol) bad |= ST_PIVOT_WEAK;
+        }
+        for (int t = tid; t < R * nb; t += nt) {
+            const int r = t / nb, c = t - r * nb;
+            if (c < w) W[(size_t)(jb + r) * ld + jb + c] = pan[t];
+        }
+        __syncthreads();
+        {
+            const long long t2 = clock64();
+            c_pan += t2 - tk;
+            tk = t2;
+        }
+        const int c1 = jb + w, ncols = D - c1;
+        if (ncols <= 0) break;
+        // U rows of the panel (triangular solve with the unit-L diagonal
+        // block), one thread per column, in groups of 8 rows so the column
+        // stays in registers.
+        for (int t = tid; t < ncols; t += nt) {
+            const size_t col = (size_t)c1 + t;
+            for (int g = 0; g < w; g += 8) {
+                double u[8];
+#pragma unroll
+                for (int r = 0; r < 8; r++) u[r] = g + r < w ? W[(size_t)(jb + g + r) * ld + col] : 0.0;
+                for (int g2 = 0; g2 < g; g2 += 8) {
+                    double v[8];
+#pragma unroll
+                    for (int c = 0; c < 8; c++) v[c] = W[(size_t)(jb + g2 + c) * ld + col];
+#pragma unroll
+                    for (int c = 0; c < 8; c++)
+#pragma unroll
+                        for (int r = 0; r < 8; r++)
+                            if (g + r < w) u[r] = __dsub_rn(u[r], __dmul_rn(pan[(g + r) * nb + g2 + c], v[c]));
+                }
+#pragma unroll
+                for (int c = 0; c < 8; c++)
+#pragma unroll
+                    for (int r = c + 1; r < 8; r++)
+                        if (g + r < w) u[r] = __dsub_rn(u[r], __dmul_rn(pan[(g + r) * nb + g + c], u[c]));
+#pragma unroll
+                for (int r = 0; r < 8; r++)
+                    if (g + r < w) W[(size_t)(jb + g + r) * ld + col] = u[r];
+            }
+        }
+        __syncthreads();
+        {
+            const long long t2 = clock64();
+            c_trsm += t2 - tk;
+            tk = t2;
+        }
+        // Trailing update W22 -= L21 U12, tiles of (4 * nty) rows x 64
+        // columns, four rows per thread, multipliers from the panel in
+        // shared memory and U12 staged per tile.
+        const int TR = 4 * nty;
+        const int nrt = (ncols + TR - 1) / TR, nct = (ncols + 63) / 64;
+        for (int tile = 0; tile < nrt * nct; tile++) {
+            const int r0 = c1 + (tile / nct) * TR, q0 = c1 + (tile % nct) * 64;
+            for (int t = tid; t < w * 64; t += nt) {
+                const int c = t >> 6, x = t & 63;
+                ut[t] = q0 + x < D ? W[(size_t)(jb + c) * ld + q0 + x] : 0.0;
+            }
+            __syncthreads();
+            const int col = q0 + tx;
+            if (col < D) {
+                double acc[4];
+                int row[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    row[q] = r0 + ty + q * nty;
+                    acc[q] = row[q] < D ? W[(size_t)row[q] * ld + col] : 0.0;
+                }
+                for (int c = 0; c < w; c++) {
+                    const double u = ut[c * 64 + tx];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int rr = min(row[q], D - 1) - jb;
+                        acc[q] = __dsub_rn(acc[q], __dmul_rn(pan[rr * nb + c], u));
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    if (row[q] < D) W[(size_t)row[q] * ld + col] = acc[q];
+            }
+            __syncthreads();
+        }
+        {
+            const long long t2 = clock64();
+            c_upd += t2 - tk;
+            tk = t2;
+        }
+    }
+    if (tid == 0) {
+        st->cyc_tpanel = c_pan;
+        st->cyc_ttrsm = c_trsm;
+        st->cyc_tupdate = c_upd;
+    }
+}
+
+// Dense trailing block -> VT storage for the solves (unit L below the
+// diagonal, U on and above) and the merged / row-major slot arrays of the
+// tail columns' rows >= k0.
+template <typename VT>
+__device__ void dense_tail_store(const SysDev& S, const PatternDev& P, const double* W, double& maxu) {
+    const int D = P.dtail, ld = P.tail_ld, k0 = P.k0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    VT* T = (VT*)S.tail;
+    for (size_t t = threadIdx.x; t < (size_t)D * ld; t += blockDim.x) {
+        const int i = (int)(t / ld), c = (int)(t - (size_t)i * ld);
+        if (c < D) {
+            const double v = W[t];
+            if (i <= c) maxu = fmax(maxu, fabs(v));
+            T[t] = ValTraits<VT>::to(v);
+        } else {
+            T[t] = ValTraits<VT>::to(0.0);
+        }
+    }
+    __syncthreads();
+    VT* lu = (VT*)S.lu;
+    VT* lval = (VT*)S.lval;
+    VT* uval = (VT*)S.uval;
+    VT* udiag = (VT*)S.udiag;
+    for (int kk = warp; kk < D; kk += nw) {
+        const int k = k0 + kk;
+        const int c0 = P.cp[k], len = P.cp[k + 1] - c0, d = P.dg[k] - c0;
+        const int* rows = P.ri + c0;
+        int below = 0;
+        for (int t = lane; t < d; t += 32) below += rows[t] < k0;
+        below = __reduce_add_sync(0xffffffffu, below);
+        for (int t = below + lane; t < len; t += 32) {
+            const VT sv = T[(size_t)(rows[t] - k0) * ld + kk];
+            lu[c0 + t] = sv;
+            const int dst = P.slot_dst[c0 + t];
+            if (t < d) uval[dst] = sv;
+            else if (t == d) udiag[k] = sv;
+            else lval[dst] = sv;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Refactorization with the pivot order and pattern frozen.
 //
 // Column k (one warp): x = A(:,k) scattered into the column's own slots
 // (duplicates summed in input order); for each U(:,k) row j ascending, once
-// column j is ready: x[i] -= L(i,j) * x[j] for the rows i of L(:,j), the
-// slot of i found by binary search in column k's sorted rows; U(:,k) =
-// x[rows < k], U(k,k) = x[k], L(:,k) = x[rows > k] / U(k,k).  The work
-// vector is fp64; multiply and subtract are separately rounded so the result
-// is bitwise reproducible on the host.  Values are stored as VT (fp32 for
-// the mixed path, fp64 for the plain path) in the merged column layout and
-// in the row-major copies used by the solves.
+// column j is ready: x[s] -= L(i,j) * x[j] for the strict-L entries (i, j),
+// s = slot of row i in column k (precomputed relative slots; a binary search
+// in column k's rows when the pattern has none); U(:,k) = x[rows < k],
+// U(k,k) = x[k], L(:,k) = x[rows > k] / U(k,k).  The work vector is fp64;
+// multiply and subtract are separately rounded so the result is bitwise
+// reproducible on the host.  Values are stored as VT (fp32 for the mixed
+// path, fp64 for the plain path) in the merged column layout and in the
+// row-major copies used by the solves.
+//
+// Shared memory per warp: x[wcap] (fp64), a stage of scap L values (VT) and
+// scap + 16 relative slots.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async_16(void* sdst, const void* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+
 template <typename VT>
 __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem_base,
                                const SolveParams& prm) {
@@ -87,18 +306,12 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
     const int n = P.n;
     Smem sm(smem_base, plan);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    // Per warp: work vector x[wcap] (fp64), staged values sval[scap] (VT),
-    // column rows wr[wcap], staged rows srow[scap].
-    double* wx = (double*)sm.uni + (size_t)warp * plan.wcap;
-    VT* sval_all = (VT*)((double*)sm.uni + (size_t)nw * plan.wcap);
-    VT* sval = sval_all + (size_t)warp * plan.scap;
-    int* wr = (int*)(sval_all + (size_t)nw * plan.scap) + (size_t)warp * plan.wcap;
-    int* srow = (int*)(sval_all + (size_t)nw * plan.scap) + (size_t)nw * plan.wcap + (size_t)warp * plan.scap;
-    // Optional per-warp row -> slot map (n entries, 16 bit).
-    unsigned short* wmap = (unsigned short*)((int*)(sval_all + (size_t)nw * plan.scap) +
-                                             (size_t)nw * (plan.wcap + plan.scap)) +
-                           (size_t)warp * plan.mcap;
-    const bool use_map = plan.mcap >= n;
+    const size_t per_warp = (size_t)plan.wcap * 8 + (size_t)plan.scap * sizeof(VT) + ((size_t)plan.scap + 16) * 2;
+    char* wbase = sm.uni + (size_t)warp * per_warp;
+    double* wx = (double*)wbase;
+    VT* sval = (VT*)(wbase + (size_t)plan.wcap * 8);
+    unsigned short* srel = (unsigned short*)(wbase + (size_t)plan.wcap * 8 + (size_t)plan.scap * sizeof(VT));
+    const bool have_rel = P.rel != nullptr && prm.refactor_mode == 0;
 
     for (int t = threadIdx.x; t < (n + 31) / 32; t += blockDim.x) sm.ready[t] = 0u;
     if (threadIdx.x == 0) {
@@ -114,6 +327,11 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         S.sell64[t] = v;
         S.sell32[t] = (float)v;
     }
+    // This CTA's dense trailing block, zeroed: the tail columns scatter only
+    // their pattern's entries into it.
+    double* W = P.dtail > 0 ? S.tailws + (size_t)blockIdx.x * S.tailws_stride : nullptr;
+    if (W)
+        for (size_t t = threadIdx.x; t < (size_t)P.dtail * P.tail_ld; t += blockDim.x) W[t] = 0.0;
     __syncthreads();
 
     VT* lu = (VT*)S.lu;
@@ -137,20 +355,26 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         const int k = P.col_order[idx];
         const int c0 = P.cp[k], c1 = P.cp[k + 1];
         const int d = P.dg[k] - c0, len = c1 - c0;
+        const int* rows = P.ri + c0;
         double* x;
-        const int* rows;
         if (len <= plan.wcap) {
             x = wx;
-            for (int t = lane; t < len; t += 32) wr[t] = P.ri[c0 + t];
-            rows = wr;
         } else if (S.scratch) {
             x = S.scratch + ((size_t)blockIdx.x * nw + warp) * P.max_col;
-            rows = P.ri + c0;
         } else {
             bad |= ST_CAPACITY;
             __syncwarp();
             if (lane == 0) set_ready(sm.ready, k);
             continue;
+        }
+        // A column of the dense trailing block applies only its dependencies
+        // before k0 here (they come first: rows ascending).
+        const bool tailcol = k >= P.k0;
+        int dsp = d;
+        if (tailcol) {
+            int below = 0;
+            for (int t = lane; t < d; t += 32) below += rows[t] < P.k0;
+            dsp = __reduce_add_sync(0xffffffffu, below);
         }
         for (int t = lane; t < len; t += 32) x[t] = 0.0;
         __syncwarp();
@@ -164,26 +388,21 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 x[dst] = s;
             }
         }
-        // Row -> slot map of this column (when the plan has room for one):
-        // entries of other rows are stale, but only rows of this column's
-        // pattern are looked up (the static pattern is closed under the
-        // updates), and map_slot verifies the hit.
-        const bool cmap = use_map && rows == wr;
-        if (cmap)
-            for (int t = lane; t < len; t += 32) wmap[rows[t]] = (unsigned short)t;
         __syncwarp();
         long long tc = clock64();
         // Apply the dependency columns in ascending order.  Each round takes
         // the next run of dependencies that are already complete (blocking
         // only when the very next one is not, so the older dependencies of a
         // column overlap with the computation of its most recent ones), up to
-        // plan.scap gathered entries; their L parts are copied to shared
-        // memory with all copies in flight together, then applied.
-        for (int u0 = 0; u0 < d;) {
+        // plan.scap gathered entries; their L values and relative slots are
+        // copied to shared memory with all copies in flight together, then
+        // applied.
+        long long roff = have_rel ? P.rel_ptr[k] : 0;   // rel index of dependency u0
+        for (int u0 = 0; u0 < dsp;) {
             const int u = u0 + lane;
             int beg = 0, cnt = 0;
             bool rdy = true;
-            if (u < d) {
+            if (u < dsp) {
                 const int jj = rows[u];
                 beg = P.dg[jj] + 1;
                 cnt = P.cp[jj + 1] - beg;
@@ -209,36 +428,40 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 if (lane >= o) incl += v;
             }
             const int excl = incl - cnt;
-            int nfit = prm.refactor_mode == 1
-                           ? 0
-                           : __popc(__ballot_sync(0xffffffffu, u < d && incl <= plan.scap));
+            int nfit = have_rel ? __popc(__ballot_sync(0xffffffffu, u < dsp && incl <= plan.scap)) : 0;
             nfit = min(nfit, nready);
             if (nfit == 0) {
-                // One dependency longer than the stage: apply it from global.
+                // One dependency applied straight from global memory (longer
+                // than the stage, or no relative slots).
                 const double xj = x[u0];
                 const int p0 = __shfl_sync(0xffffffffu, beg, 0);
-                const int p1 = p0 + __shfl_sync(0xffffffffu, cnt, 0);
+                const int c = __shfl_sync(0xffffffffu, cnt, 0);
                 if (xj != 0.0) {
-                    for (int p = p0 + lane; p < p1; p += 32) {
-                        const int i = P.ri[p];
-                        const double l = ValTraits<VT>::load(lu + p);
-                        const int s = cmap ? map_slot(wmap, rows, len, i) : find_slot(rows, u0 + 1, len, i);
+                    for (int e = lane; e < c; e += 32) {
+                        const double l = ValTraits<VT>::load(lu + p0 + e);
+                        const int s = have_rel ? (int)P.rel[roff + e]
+                                               : find_slot(rows, u0 + 1, len, P.ri[p0 + e]);
                         if (s >= 0) x[s] = __dsub_rn(x[s], __dmul_rn(l, xj));
                         else bad |= ST_CAPACITY;
                     }
                 }
                 __syncwarp();
+                roff += c;
                 u0 += 1;
                 continue;
             }
+            // Stage: relative slots of the round (one contiguous run of rel,
+            // copied in aligned 16-byte pieces) and each dependency's values.
+            const int tot = __shfl_sync(0xffffffffu, incl, nfit - 1);
+            const long long g0 = roff & ~7LL;
+            const int sh = (int)(roff - g0);
+            const int pieces = (sh + tot + 7) >> 3;
+            for (int e = lane; e < pieces; e += 32) cp_async_16(srel + 8 * e, P.rel + g0 + 8 * e);
             for (int t = 0; t < nfit; t++) {
                 const int b_t = __shfl_sync(0xffffffffu, beg, t);
                 const int c_t = __shfl_sync(0xffffffffu, cnt, t);
                 const int o_t = __shfl_sync(0xffffffffu, excl, t);
-                for (int e = lane; e < c_t; e += 32) {
-                    cp_async_4(srow + o_t + e, P.ri + b_t + e);
-                    cp_async_val(sval + o_t + e, lu + b_t + e);
-                }
+                for (int e = lane; e < c_t; e += 32) cp_async_val(sval + o_t + e, lu + b_t + e);
             }
             cp_async_wait_all();
             __syncwarp();
@@ -250,15 +473,24 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
             for (int t = 0; t < nfit; t++) {
                 const int c_t = __shfl_sync(0xffffffffu, cnt, t);
                 const int o_t = __shfl_sync(0xffffffffu, excl, t);
-                const int uu = u0 + t;
-                const double xj = x[uu];
+                const double xj = x[u0 + t];
                 if (xj != 0.0) {
-                    for (int e = lane; e < c_t; e += 32) {
-                        const int i = srow[o_t + e];
-                        const double l = ValTraits<VT>::load(sval + o_t + e);
-                        const int s = cmap ? map_slot(wmap, rows, len, i) : find_slot(rows, uu + 1, len, i);
-                        if (s >= 0) x[s] = __dsub_rn(x[s], __dmul_rn(l, xj));
-                        else bad |= ST_CAPACITY;
+                    // Rows of one dependency are distinct: four entries per
+                    // lane are loaded before any is written back.
+                    for (int e = lane; e < c_t; e += 128) {
+                        int s[4];
+                        double l[4], xv[4];
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            const int ee = e + 32 * q;
+                            s[q] = ee < c_t ? (int)srel[sh + o_t + ee] : -1;
+                            l[q] = ee < c_t ? ValTraits<VT>::load(sval + o_t + ee) : 0.0;
+                        }
+#pragma unroll
+                        for (int q = 0; q < 4; q++) xv[q] = s[q] >= 0 ? x[s[q]] : 0.0;
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            if (s[q] >= 0) x[s[q]] = __dsub_rn(xv[q], __dmul_rn(l[q], xj));
                     }
                 }
                 __syncwarp();
@@ -268,7 +500,24 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 c_update += t2 - tc;
                 tc = t2;
             }
+            roff += tot;
             u0 += nfit;
+        }
+        if (tailcol) {
+            // U rows before k0 are final; the rest goes to the dense block.
+            for (int t = lane; t < len; t += 32) {
+                const double v = x[t];
+                if (t < dsp) {
+                    maxu = fmax(maxu, fabs(v));
+                    const VT sv = ValTraits<VT>::to(v);
+                    lu[c0 + t] = sv;
+                    uval[P.slot_dst[c0 + t]] = sv;
+                } else {
+                    W[(size_t)(rows[t] - P.k0) * P.tail_ld + (k - P.k0)] = v;
+                }
+            }
+            __syncwarp();
+            continue;
         }
         const double piv = x[d];
         double amax = 0.0;
@@ -300,6 +549,12 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         if (lane == 0) set_ready(sm.ready, k);
     }
 
+    if (W) {
+        __syncthreads();
+        dense_tail_factor<VT>(P, W, sm, plan, prm, minpiv, minratio, bad, S.stats);
+        __syncthreads();
+        dense_tail_store<VT>(S, P, W, maxu);
+    }
     if (lane == 0) {
         atomicAdd((unsigned long long*)&S.stats->cyc_wait, (unsigned long long)c_wait);
         atomicAdd((unsigned long long*)&S.stats->cyc_gather, (unsigned long long)c_gather);
@@ -347,15 +602,122 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
 }
 
 // ---------------------------------------------------------------------------
+// Triangular solves of the dense trailing block (rows [k0, n), factor T in
+// VT with leading dimension ld): 32-row blocks, the diagonal block by one
+// warp through shuffles, the rest of the block's columns as one
+// multiply-add per row and thread.  fp64 accumulation.
+// ---------------------------------------------------------------------------
+// sum_{c < w} row[c] * y[c] for one 32-column block of a tail row: all
+// loads issued before the multiply-adds.
+template <typename VT>
+__device__ __forceinline__ double tail_row_dot(const VT* row, const double* y, int w) {
+    VT v[32];
+#pragma unroll
+    for (int c = 0; c < 32; c++) v[c] = c < w ? row[c] : VT(0);
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 32; c++)
+        if (c < w) acc = fma((double)v[c], y[c], acc);
+    return acc;
+}
+
+// y[k0..n) := L_tt^-1 (y - L_ts y_s): first the tail rows' entries in the
+// columns before k0, then the unit-lower dense solve.
+template <typename VT>
+__device__ void tail_forward(const PatternDev& P, const VT* lval, const VT* T, double* y) {
+    const int n = P.n, k0 = P.k0, D = P.dtail, ld = P.tail_ld;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = k0 + warp; i < n; i += nw) {
+        // Tail rows sit at sweep index i; their entries ascend by column.
+        const int p0 = P.lrp[i], p1 = P.lrp[i + 1];
+        double acc = 0.0;
+        int p = p0 + lane;
+        for (; p + 96 < p1; p += 128) {
+            int jj[4];
+            double vv[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                jj[q] = P.lci[p + 32 * q];
+                vv[q] = ValTraits<VT>::load(lval + p + 32 * q);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (jj[q] < k0) acc = fma(vv[q], y[jj[q]], acc);
+        }
+        for (; p < p1; p += 32) {
+            const int j = P.lci[p];
+            if (j < k0) acc = fma(ValTraits<VT>::load(lval + p), y[j], acc);
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) y[i] -= acc;
+    }
+    __syncthreads();
+    double* yt = y + k0;
+    for (int jb = 0; jb < D; jb += 32) {
+        const int w = min(32, D - jb);
+        if (warp == 0) {
+            double lr[32];
+            const VT* row = T + (size_t)(jb + lane) * ld + jb;
+#pragma unroll
+            for (int c = 0; c < 32; c++) lr[c] = (c < lane && lane < w) ? ValTraits<VT>::load(row + c) : 0.0;
+            double yr = lane < w ? yt[jb + lane] : 0.0;
+#pragma unroll
+            for (int c = 0; c < 31; c++) {
+                const double yc = __shfl_sync(0xffffffffu, yr, c);
+                if (c < lane) yr = fma(-lr[c], yc, yr);
+            }
+            if (lane < w) yt[jb + lane] = yr;
+        }
+        __syncthreads();
+        for (int i = jb + w + threadIdx.x; i < D; i += blockDim.x)
+            yt[i] -= tail_row_dot<VT>(T + (size_t)i * ld + jb, yt + jb, w);
+        __syncthreads();
+    }
+}
+
+// y[k0..n) := U_tt^-1 y[k0..n) (upper with diagonal).
+template <typename VT>
+__device__ void tail_backward(const PatternDev& P, const VT* T, double* y) {
+    const int k0 = P.k0, D = P.dtail, ld = P.tail_ld;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* yt = y + k0;
+    for (int jb = ((D - 1) / 32) * 32; jb >= 0; jb -= 32) {
+        const int w = min(32, D - jb);
+        if (warp == 0) {
+            double ur[32];
+            const VT* row = T + (size_t)(jb + lane) * ld + jb;
+#pragma unroll
+            for (int c = 0; c < 32; c++) ur[c] = (c > lane && c < w) ? ValTraits<VT>::load(row + c) : 0.0;
+            const double dg = lane < w ? ValTraits<VT>::load(row + lane) : 1.0;
+            double yr = lane < w ? yt[jb + lane] : 0.0;
+#pragma unroll
+            for (int c = 31; c >= 0; c--) {
+                if (c < w) {
+                    if (lane == c) yr = yr / dg;
+                    const double zc = __shfl_sync(0xffffffffu, yr, c);
+                    if (lane < c) yr = fma(-ur[c], zc, yr);
+                }
+            }
+            if (lane < w) yt[jb + lane] = yr;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < jb; i += blockDim.x)
+            yt[i] -= tail_row_dot<VT>(T + (size_t)i * ld + jb, yt + jb, w);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // y := U^-1 L^-1 rhs in pivot-position space (level-scheduled, warp per row,
 // factors read as VT, accumulation in fp64).  y may be shared or global
 // memory; rhs must not alias y.
 // ---------------------------------------------------------------------------
 template <typename VT>
 __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval,
-                             const VT* udiag, const double* rhs, double* y, Smem& sm,
-                             int& bad) {
-    const int n = P.n;
+                             const VT* udiag, const VT* tail, const double* rhs, double* y, Smem& sm,
+                             int& bad, SysStats* st) {
+    const long long t0 = clock64();
+    const int n = P.n, k0 = P.k0;
     const int lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = rhs[i];
     for (int t = threadIdx.x; t < (n + 31) / 32; t += blockDim.x) sm.ready[t] = 0u;
@@ -367,7 +729,7 @@ __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval
     volatile double* vy = y;
     while (true) {
         const int idx = warp_claim(&sm.ctl[0]);
-        if (idx >= n) break;
+        if (idx >= k0) break;
         const int i = P.fwd_order[idx];
         const int p0 = P.lrp[idx], p1 = P.lrp[idx + 1];
         double acc = 0.0;
@@ -386,12 +748,25 @@ __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval
         }
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < (n + 31) / 32; t += blockDim.x) sm.ready[t] = 0u;
+    const long long t1 = clock64();
+    if (P.dtail > 0) {
+        tail_forward<VT>(P, lval, tail, y);
+        tail_backward<VT>(P, tail, y);
+    }
+    const long long t2 = clock64();
+    // Rows of the dense tail are complete before the sparse U sweep starts.
+    for (int t = threadIdx.x; t < (n + 31) / 32; t += blockDim.x) {
+        const int lo = t * 32;
+        unsigned bits = 0u;
+        for (int b = 0; b < 32; b++)
+            if (lo + b >= k0 && lo + b < n) bits |= 1u << b;
+        sm.ready[t] = bits;
+    }
     if (threadIdx.x == 0) sm.ctl[0] = 0;
     __syncthreads();
     while (true) {
         const int idx = warp_claim(&sm.ctl[0]);
-        if (idx >= n) break;
+        if (idx >= k0) break;
         const int i = P.bwd_order[idx];
         const int p0 = P.urp[idx], p1 = P.urp[idx + 1];
         double acc = 0.0;
@@ -410,6 +785,11 @@ __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval
         }
     }
     __syncthreads();
+    if (threadIdx.x == 0 && st) {
+        st->cyc_lsolve += t1 - t0;
+        st->cyc_tail += t2 - t1;
+        st->cyc_usolve += clock64() - t2;
+    }
 }
 
 // One triangular sweep, level-synchronous: the rows of a level are spread
@@ -456,8 +836,17 @@ __device__ void level_sweep(int nlev, const int* lev, const int* order, const in
         const int i = order[IDX];                                                 \
         const int p1 = rp[IDX + 1];                                               \
         double acc = COL >= 0 ? V * y[COL] : 0.0;                                 \
-        for (int p = rp[IDX] + 32 + lane; p < p1; p += 32)                        \
-            acc = fma(ValTraits<VT>::load(val + p), y[ci[p]], acc);               \
+        int p = rp[IDX] + 32 + lane;                                              \
+        for (; p + 96 < p1; p += 128) {                                           \
+            int cc[4];                                                            \
+            double vv[4];                                                         \
+            _Pragma("unroll") for (int q = 0; q < 4; q++) {                       \
+                cc[q] = ci[p + 32 * q];                                           \
+                vv[q] = ValTraits<VT>::load(val + p + 32 * q);                    \
+            }                                                                     \
+            _Pragma("unroll") for (int q = 0; q < 4; q++) acc = fma(vv[q], y[cc[q]], acc); \
+        }                                                                         \
+        for (; p < p1; p += 32) acc = fma(ValTraits<VT>::load(val + p), y[ci[p]], acc); \
         acc = warp_sum(acc);                                                      \
         if (lane == 0) y[i] = UPPER ? (y[i] - acc) / D : y[i] - acc;              \
     }
@@ -513,7 +902,8 @@ __device__ void load_sweep_desc(const PatternDev& P, int* d) {
 // in shared memory at d).
 template <typename VT>
 __device__ void cta_lu_apply_levels(const PatternDev& P, const VT* lval, const VT* uval,
-                                    const VT* udiag, const double* rhs, double* y, const int* d) {
+                                    const VT* udiag, const VT* tail, const double* rhs, double* y,
+                                    const int* d, SysStats* st) {
     const int n = P.n, nfl = P.nfwd_levels, nbl = P.nbwd_levels;
     const int* f_ord = d;
     const int* f_rp = f_ord + n;
@@ -523,18 +913,32 @@ __device__ void cta_lu_apply_levels(const PatternDev& P, const VT* lval, const V
     const int* b_lev = b_rp + n + 1;
     for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = rhs[i];
     __syncthreads();
+    const long long t0 = clock64();
     level_sweep<VT, false>(nfl, f_lev, f_ord, f_rp, P.lci, lval, udiag, y);
+    __syncthreads();
+    const long long t1 = clock64();
+    if (P.dtail > 0) {
+        tail_forward<VT>(P, lval, tail, y);
+        tail_backward<VT>(P, tail, y);
+    }
+    const long long t2 = clock64();
     level_sweep<VT, true>(nbl, b_lev, b_ord, b_rp, P.uci, uval, udiag, y);
+    __syncthreads();
+    if (threadIdx.x == 0 && st) {
+        st->cyc_lsolve += t1 - t0;
+        st->cyc_tail += t2 - t1;
+        st->cyc_usolve += clock64() - t2;
+    }
 }
 
 // Dispatch: level-synchronous sweeps when their descriptors sit in shared
 // memory (desc != nullptr), else the dataflow version.
 template <typename VT>
 __device__ __forceinline__ void lu_apply(const PatternDev& P, const VT* lval, const VT* uval,
-                                         const VT* udiag, const double* rhs, double* y,
-                                         Smem& sm, const int* desc, int& bad) {
-    if (desc) cta_lu_apply_levels<VT>(P, lval, uval, udiag, rhs, y, desc);
-    else cta_lu_apply<VT>(P, lval, uval, udiag, rhs, y, sm, bad);
+                                         const VT* udiag, const VT* tail, const double* rhs, double* y,
+                                         Smem& sm, const int* desc, int& bad, SysStats* st) {
+    if (desc) cta_lu_apply_levels<VT>(P, lval, uval, udiag, tail, rhs, y, desc, st);
+    else cta_lu_apply<VT>(P, lval, uval, udiag, tail, rhs, y, sm, bad, st);
 }
 
 // out = A x (RESID: out = bt - A x) with A in SELL-C-sigma, C = 32, values AT.
@@ -584,7 +988,7 @@ __device__ void direct_phase(const SysDev& S, const SmemPlan& plan, char* smem_b
         desc = d;
     }
     const double nb = sqrt(cta_dot(bt, bt, n, sm));
-    lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, bt, y, sm, desc, bad);
+    lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, (const VT*)S.tail, bt, y, sm, desc, bad, S.stats);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         xt[i] = y[i];
         S.x[P.q[i]] = y[i];
@@ -641,6 +1045,7 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
     const VT* lval = (const VT*)S.lval;
     const VT* uval = (const VT*)S.uval;
     const VT* udiag = (const VT*)S.udiag;
+    const VT* tail = (const VT*)S.tail;
     const AT* ainner = (const AT*)(sizeof(AT) == 8 ? (const void*)S.sell64 : (const void*)S.sell32);
     int bad = 0;
     int status = 0;
@@ -714,9 +1119,11 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         int jj = 0;
         for (int j = 0; j < m; j++) {
             const double* vj = V + (size_t)j * n;
-            lu_apply<VT>(P, lval, uval, udiag, vj, y, sm, desc, bad);
+            lu_apply<VT>(P, lval, uval, udiag, tail, vj, y, sm, desc, bad, S.stats);
+            const long long tsp = clock64();
             cta_spmv<AT, false>(P, ainner, y, nullptr, w);
             __syncthreads();
+            if (threadIdx.x == 0) S.stats->cyc_spmv += clock64() - tsp;
             const double wn0 = sqrt(cta_dot(w, w, n, sm));
             for (int pass = 0; pass < 2; pass++) {
                 for (int i = warp; i <= j; i += nw) {
@@ -783,7 +1190,7 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
             z[e] = acc;
         }
         __syncthreads();
-        lu_apply<VT>(P, lval, uval, udiag, z, y, sm, desc, bad);
+        lu_apply<VT>(P, lval, uval, udiag, tail, z, y, sm, desc, bad, S.stats);
         double sy = 0.0, sx = 0.0;
         for (int e = threadIdx.x; e < n; e += blockDim.x) {
             xprev[e] = xt[e];

@@ -243,7 +243,6 @@ bool ServerObj::try_launch(Flight& f) {
     std::vector<Request*> pick;
     std::vector<PatternObj*> pats;
     size_t up_bytes = 0, down_bytes = 0, priv = 0;
-    int colmax = 0;
     const int maxb = std::max(1, opts.max_batch);
     for (Request* r : queue) {
         if ((int)pick.size() >= maxb) break;
@@ -276,24 +275,60 @@ bool ServerObj::try_launch(Flight& f) {
         up_bytes += up;
         down_bytes += down;
         priv += pv;
-        colmax = std::max(colmax, S.max_col);
     }
     if (pick.empty()) return false;
-    const int ns = (int)pick.size();
+    // Launch shapes and arena layout; drop requests from the back of the
+    // pick until everything (including the refactor spill area) fits.
     SmemPlan plan;
-    if (plan_for(pats, o, plan) != LUSP_OK) {
-        o.solve_sweep = 0;
-        plan_for(pats, o, plan);
+    LaunchArgs la;
+    int grid = 0;
+    size_t nval = 0, nvec = 0, spill = 0, tws = 0, tail_bytes = 0;
+    while (true) {
+        const int nsp = (int)pick.size();
+        nval = nvec = 0;
+        size_t privs = 0;
+        int cm = 0;
+        for (Request* r : pick) {
+            nval += r->vals.size();
+            nvec += r->rhs.size();
+            privs += system_private_bytes(r->pe->pat->S, vs, o.krylov);
+            cm = std::max(cm, r->pe->pat->S.max_col);
+        }
+        if (plan_for(pats, o, plan) != LUSP_OK) {
+            o.solve_sweep = 0;
+            plan_for(pats, o, plan);
+        }
+        int occ = 0;
+        if (kernel_occupancy(o.prec, o.inner_prec, plan.bytes, o.block_threads, &occ) != LUSP_OK || occ < 1)
+            return false;
+        grid = std::min(nsp, occ * sm_count());
+        if (refactor_setup(pats, o, nsp, la) != LUSP_OK) return false;
+        spill = spill_bytes(la.rgrid, la.rblock, cm, la.rplan);
+        tws = tail_work_doubles(pats);
+        tail_bytes = al((size_t)la.rgrid * tws * 8);
+        const size_t total = al(nval * 8) + 2 * al(nvec * 8) + privs + spill + tail_bytes +
+                             al(sizeof(SysStats) * nsp) +
+                             al(sizeof(SysDev) * nsp) + 256;
+        if (total <= f.arena_bytes) break;
+        if (nsp == 1) {
+            Request* r = pick[0];
+            r->res.rc = LUSP_EALLOC;
+            r->res.status = LUSP_ST_CAPACITY;
+            r->t_done = Clock::now();
+            r->res.latency_ms = ms_since(r->t_submit, r->t_done);
+            r->done = true;
+            r->pe->users--;
+            stats.completed++;
+            queue.erase(std::find(queue.begin(), queue.end(), r));
+            cv_done.notify_all();
+            return true;
+        }
+        pick.pop_back();
+        pats.pop_back();
     }
-    int occ = 0;
-    if (kernel_occupancy(o.prec, o.inner_prec, plan.bytes, o.block_threads, &occ) != LUSP_OK || occ < 1) return false;
-    const int grid = std::min(ns, occ * sm_count());
-    // Arena layout: values | rhs | x | per-system private | spill | stats | descriptors | queue.
-    size_t nval = 0, nvec = 0;
-    for (Request* r : pick) {
-        nval += r->vals.size();
-        nvec += r->rhs.size();
-    }
+    const int ns = (int)pick.size();
+    // Arena layout: values | rhs | x | per-system private | spill | tail work | stats |
+    // descriptors | queue.
     char* a = f.arena;
     double* d_vals = (double*)a;
     double* d_rhs = (double*)(a + al(nval * 8));
@@ -314,9 +349,10 @@ bool ServerObj::try_launch(Flight& f) {
         ov += r->vals.size();
         ob += r->rhs.size();
     }
-    const size_t spill = spill_bytes(grid, o.block_threads, colmax, plan);
     double* d_spill = spill ? (double*)p : nullptr;
     p += spill;
+    double* d_tailws = tws ? (double*)p : nullptr;
+    p += tail_bytes;
     SysStats* d_stats = (SysStats*)p;
     p += al(sizeof(SysStats) * ns);
     SysDev* d_sys = (SysDev*)p;
@@ -326,6 +362,8 @@ bool ServerObj::try_launch(Flight& f) {
     if ((size_t)(p - a) > f.arena_bytes) return false;
     for (int i = 0; i < ns; i++) {
         hs[i].scratch = d_spill;
+        hs[i].tailws = d_tailws;
+        hs[i].tailws_stride = (long long)tws;
         hs[i].stats = d_stats + i;
     }
     // Stage the inputs in pinned memory and move them in one copy.
@@ -348,7 +386,6 @@ bool ServerObj::try_launch(Flight& f) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_rhs, up + rhs_at, nvec * 8, cudaMemcpyHostToDevice, f.st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_sys, hs.data(), sizeof(SysDev) * ns, cudaMemcpyHostToDevice, f.st);
     if (e != cudaSuccess) return false;
-    LaunchArgs la;
     la.d_sys = d_sys;
     la.nsys = ns;
     la.d_queue = d_queue;

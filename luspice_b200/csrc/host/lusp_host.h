@@ -76,12 +76,37 @@ struct StaticPattern {
     int max_col = 0;                // longest merged column (slots)
     long flops = 0;                 // multiply-adds of one refactorization
     long gathered = 0;              // sum over deps of |L(:,j)| (entries)
+
+    // Relative slots of the refactorization updates: for column k, for each
+    // dependency j (rows of U(:,k) ascending), for each strict-L entry of
+    // column j in storage order, the slot offset inside column k that the
+    // entry updates.  Column k's list is rel[rel_ptr[k] .. rel_ptr[k+1]).
+    // Empty when a column is longer than 65535 slots.
+    std::vector<uint16_t> rel;
+    std::vector<long long> rel_ptr;
+
+    // Dense trailing block: rows and columns [k0, n) are refactored and
+    // solved as one dense D x D block (D = dtail = n - k0; 0 = none).  The
+    // sweep orders then list the rows < k0 level-sorted (nfwd_levels /
+    // nbwd_levels count these levels only), followed by the tail rows in
+    // ascending order.
+    int k0 = 0, dtail = 0;
 };
+
+// Largest dense trailing block.
+constexpr int kMaxDenseTail = 768;
 
 // Build the static layout from a pivot factorization.  Ap/Ai is the same
 // CSC (original indices) the factorization consumed.
+// dense_tail: -1 chooses the trailing block size by a cost model, 0 none,
+// > 0 that many trailing columns (at most kMaxDenseTail and n).
 void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
-                          const PivotFactor& F, int sell_sigma, StaticPattern& S);
+                          const PivotFactor& F, int sell_sigma, StaticPattern& S,
+                          int dense_tail = -1);
+
+// Trailing block size the cost model picks for a merged pattern whose
+// columns, levels and update counts are already set.
+int choose_dense_tail(const StaticPattern& S);
 
 uint64_t pattern_hash(int n, const int* Ap, const int* Ai, const int* q);
 

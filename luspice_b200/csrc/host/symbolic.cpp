@@ -203,8 +203,43 @@ void levels_and_order(int n, const std::vector<int>& visit,
 
 }  // namespace
 
+// Trailing block size by a cost model in SM cycles of one refactor plus the
+// triangular solves of one GMRES-IR solve.  The sparse engine costs about a
+// cycle per gathered update plus a latency per level of the column schedule
+// (and of the solve sweeps, which have a similar depth); the dense block
+// costs its multiply-subtract pairs (D^3 / 3) plus a latency per 32-column
+// panel (the panel's own dependency chain and the blocked solves).
+int choose_dense_tail(const StaticPattern& S) {
+    const int n = S.n;
+    if (n < 32) return 0;
+    const double c_upd = 1.0, c_lev = 18000.0, c_pair = 0.05, c_panel = 56000.0;
+    // Updates that stay in the sparse engine for a tail starting at k0:
+    // those whose dependency column j lies before k0.  Column j feeds
+    // |L(:,j)| updates into each of the |U(j,:)| later columns.
+    std::vector<long> urow(n, 0);
+    for (int k = 0; k < n; k++)
+        for (int p = S.cp[k]; p < S.dg[k]; p++) urow[S.ri[p]]++;
+    std::vector<double> inside(n + 1, 0.0);   // updates with j >= k0
+    for (int j = n - 1; j >= 0; j--)
+        inside[j] = inside[j + 1] + (double)(S.cp[j + 1] - S.dg[j] - 1) * (double)urow[j];
+    std::vector<int> levmax(n + 1, 0);        // levels of the columns < k0
+    for (int k = 0; k < n; k++) levmax[k + 1] = std::max(levmax[k], S.col_level[k] + 1);
+    double best = c_upd * (double)S.gathered + c_lev * S.ncol_levels;
+    int best_d = 0;
+    for (int D = 32; D <= std::min(n, kMaxDenseTail); D += 32) {
+        const int k0 = n - D;
+        const double cost = c_upd * ((double)S.gathered - inside[k0]) + c_lev * levmax[k0] +
+                            c_pair * (double)D * D * D / 3.0 + c_panel * ((D + 31) / 32);
+        if (cost < best) {
+            best = cost;
+            best_d = D;
+        }
+    }
+    return best_d;
+}
+
 void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
-                          const PivotFactor& F, int sell_sigma, StaticPattern& S) {
+                          const PivotFactor& F, int sell_sigma, StaticPattern& S, int dense_tail) {
     S.n = n;
     S.nnz_a = Ap[n];
     S.lnnz = F.Lp[n];
@@ -269,6 +304,43 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         S.gathered = ga;
     }
 
+    // Relative update slots (16 bit), built through a row -> slot table of
+    // the current column.
+    S.rel.clear();
+    S.rel_ptr.clear();
+    if (S.max_col <= 65535) {
+        S.rel.reserve((size_t)S.gathered);
+        S.rel_ptr.assign(n + 1, 0);
+        std::vector<int> at(n, -1);
+        bool closed = true;
+        for (int k = 0; k < n && closed; k++) {
+            S.rel_ptr[k] = (long long)S.rel.size();
+            for (int p = S.cp[k]; p < S.cp[k + 1]; p++) at[S.ri[p]] = p - S.cp[k];
+            for (int p = S.cp[k]; p < S.dg[k]; p++) {
+                const int j = S.ri[p];
+                for (int t = S.dg[j] + 1; t < S.cp[j + 1]; t++) {
+                    const int s = at[S.ri[t]];
+                    if (s < 0) closed = false;   // pattern not closed under the updates
+                    S.rel.push_back((uint16_t)s);
+                }
+            }
+            for (int p = S.cp[k]; p < S.cp[k + 1]; p++) at[S.ri[p]] = -1;
+        }
+        S.rel_ptr[n] = (long long)S.rel.size();
+        if (!closed) {
+            S.rel.clear();
+            S.rel_ptr.clear();
+        }
+    }
+
+    // Dense trailing block.
+    {
+        int D = dense_tail < 0 ? choose_dense_tail(S) : dense_tail;
+        D = std::max(0, std::min({D, n, kMaxDenseTail}));
+        S.dtail = D;
+        S.k0 = n - D;
+    }
+
     // Row-major copies of strict L and strict U.
     {
         S.lrp.assign(n + 1, 0);
@@ -302,15 +374,29 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
                 S.slot_dst[p] = d;
             }
         }
-        // Forward levels: row i depends on columns of its L row (all < i).
-        std::vector<int> visit(n);
+        // Sweep orders over the rows before the dense tail (all rows when
+        // there is none); the tail rows follow in ascending order.
+        const int k0 = S.k0;
+        // Forward levels: row i depends on the columns of its L row (< i).
+        std::vector<int> visit(k0);
         std::iota(visit.begin(), visit.end(), 0);
         std::vector<int> lev;
-        levels_and_order(n, visit, S.lrp, S.lci, lev, S.fwd_order, S.nfwd_levels, &S.fwd_lev);
-        // Backward levels: row i depends on columns of its U row (all > i).
-        std::vector<int> rvisit(n);
-        for (int i = 0; i < n; i++) rvisit[i] = n - 1 - i;
-        levels_and_order(n, rvisit, S.urp, S.uci, lev, S.bwd_order, S.nbwd_levels, &S.bwd_lev);
+        levels_and_order(k0, visit, S.lrp, S.lci, lev, S.fwd_order, S.nfwd_levels, &S.fwd_lev);
+        // Backward levels: row i depends on the columns of its U row (> i)
+        // that lie before the tail (the tail is solved first).
+        std::vector<int> bptr(k0 + 1, 0), bdep;
+        for (int i = 0; i < k0; i++) {
+            for (int p = S.urp[i]; p < S.urp[i + 1]; p++)
+                if (S.uci[p] < k0) bdep.push_back(S.uci[p]);
+            bptr[i + 1] = (int)bdep.size();
+        }
+        std::vector<int> rvisit(k0);
+        for (int i = 0; i < k0; i++) rvisit[i] = k0 - 1 - i;
+        levels_and_order(k0, rvisit, bptr, bdep, lev, S.bwd_order, S.nbwd_levels, &S.bwd_lev);
+        for (int i = k0; i < n; i++) {
+            S.fwd_order.push_back(i);
+            S.bwd_order.push_back(i);
+        }
         // Store the rows contiguously in level order: row fwd_order[idx] of L
         // occupies [lrp[idx], lrp[idx+1]) (U likewise with bwd_order), so a
         // sweep streams through memory in the order it consumes it.
