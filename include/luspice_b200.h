@@ -89,6 +89,9 @@ typedef struct {
     /* SM cycles of the refactor's dense trailing block: panels, U-row
      * solves, trailing updates */
     long long cyc_tpanel, cyc_ttrsm, cyc_tupdate;
+    /* SM cycles of the dense-tail solves: diagonal-block chains, products
+     * with the block columns */
+    long long cyc_tdiag, cyc_tgemv;
 } lusp_sys_stats;
 
 typedef struct {
@@ -99,8 +102,10 @@ typedef struct {
     double inner_rel;              /* inner stop vs current residual (default 1e-8) */
     double stag_ratio;             /* required residual reduction per outer (default 0.5) */
     double pivot_tol;              /* frozen-pivot acceptance (default 1e-3) */
-    int block_threads;             /* CTA size of the solve kernel (default 256) */
-    int ctas_per_sm;               /* solve kernel shared-memory plan target (default 2) */
+    int block_threads;             /* CTA size of the solve kernel: 0 auto (512 when the
+                                      batch has at most one system per SM, else 256) */
+    int ctas_per_sm;               /* solve kernel shared-memory plan target: 0 auto
+                                      (1 or 2 with the same rule) */
     int solve_sweep;               /* triangular solves: 0 auto, 1 dataflow (per-row
                                       ready bits), 2 level-synchronous (barrier per
                                       level, descriptors in shared memory) */

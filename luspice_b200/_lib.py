@@ -32,7 +32,8 @@ class SysStats(C.Structure):
                 ("cyc_gather", C.c_longlong), ("cyc_update", C.c_longlong), ("cyc_refactor", C.c_longlong),
                 ("cyc_lsolve", C.c_longlong), ("cyc_tail", C.c_longlong), ("cyc_usolve", C.c_longlong),
                 ("cyc_spmv", C.c_longlong), ("cyc_solve", C.c_longlong), ("cyc_tpanel", C.c_longlong),
-                ("cyc_ttrsm", C.c_longlong), ("cyc_tupdate", C.c_longlong)]
+                ("cyc_ttrsm", C.c_longlong), ("cyc_tupdate", C.c_longlong), ("cyc_tdiag", C.c_longlong),
+                ("cyc_tgemv", C.c_longlong)]
 
 
 class BatchOpts(C.Structure):

@@ -154,8 +154,8 @@ void lusp_batch_opts_default(lusp_batch_opts* o) {
     o->inner_rel = 1e-8;
     o->stag_ratio = 0.5;
     o->pivot_tol = 1e-3;
-    o->block_threads = 256;
-    o->ctas_per_sm = 2;
+    o->block_threads = 0;
+    o->ctas_per_sm = 0;
     o->solve_sweep = 0;
     o->refactor_mode = 0;
     o->inner_prec = 0;
@@ -246,7 +246,7 @@ int lusp_batch_run_graph(lusp_batch* hb, int what, void* stream) {
     }
     cudaError_t e = cudaGraphLaunch(it->second.exec, st);
     if (e != cudaSuccess) return lusp::cuda_fail(e, "graph launch");
-    B->launches = lusp::launch_kernel_count(what);
+    B->launches = lusp::launch_kernel_count(B->launch, what);
     return LUSP_OK;
 }
 

@@ -46,9 +46,10 @@ int cuda_fail(cudaError_t e, const char* what) {
 // ---------------------------------------------------------------------------
 // The persistent kernels: every CTA takes systems from a device work queue
 // until it is empty.  The refactorization runs as its own kernel (many warps
-// per CTA, few registers each); the solve kernel runs the triangular solves
-// and GMRES-IR (fewer warps, more registers).  queue[0] feeds the refactor
-// kernel, queue[1] the solve kernel.
+// per CTA, few registers each), the dense trailing blocks as a second (few
+// warps, many registers), the triangular solves and GMRES-IR as a third.
+// queue[0] feeds the refactor kernel, queue[1] the solve kernel, queue[2]
+// the dense kernel.
 // ---------------------------------------------------------------------------
 template <typename VT>
 __global__ void __launch_bounds__(1024, 1)
@@ -63,6 +64,22 @@ refactor_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan p
         if (t >= nsys) break;
         const SysDev S = sys[t];
         refactor_phase<VT>(S, plan, smem, prm);
+    }
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(512, 1)
+dense_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan, SolveParams prm) {
+    extern __shared__ __align__(16) char smem[];
+    __shared__ int s_task;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_task = atomicAdd(queue + 2, 1);
+        __syncthreads();
+        const int t = s_task;
+        if (t >= nsys) break;
+        const SysDev S = sys[t];
+        dense_phase<VT>(S, plan, smem, prm);
     }
 }
 
@@ -85,6 +102,8 @@ solve_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan
             S.stats->cyc_tail = 0;
             S.stats->cyc_usolve = 0;
             S.stats->cyc_spmv = 0;
+            S.stats->cyc_tdiag = 0;
+            S.stats->cyc_tgemv = 0;
         }
         __syncthreads();
         if (direct) direct_phase<VT>(S, plan, smem);
@@ -162,10 +181,13 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     const std::vector<int>* arrays[] = {&S.cp, &S.ri, &S.dg, &S.col_order, &S.a_ptr, &S.a_src, &S.a_dst,
                                         &S.lrp, &S.lci, &S.urp, &S.uci, &S.slot_dst, &S.fwd_order,
                                         &S.bwd_order, &S.sell_ptr, &S.sell_col, &S.sell_src,
-                                        &S.sell_perm, &S.rowat, &S.q, &S.fwd_lev, &S.bwd_lev};
+                                        &S.sell_perm, &S.rowat, &S.q, &S.fwd_lev, &S.bwd_lev, &S.bwd_pos,
+                                        &S.fwd_ldesc, &S.bwd_ldesc};
     const int narr = (int)(sizeof(arrays) / sizeof(arrays[0]));
     std::vector<size_t> off(narr + 1, 0);
-    for (int a = 0; a < narr; a++) off[a + 1] = off[a] + ((arrays[a]->size() + 31) & ~(size_t)31);
+    // Each array gets at least 8 ints of slack: the sweeps copy index runs
+    // in aligned 16-byte pieces that may end up to 3 entries past a run.
+    for (int a = 0; a < narr; a++) off[a + 1] = off[a] + ((arrays[a]->size() + 8 + 31) & ~(size_t)31);
     int* blk = nullptr;
     cudaError_t e = cudaMalloc(&blk, std::max<size_t>(off[narr], 32) * sizeof(int));
     if (e != cudaSuccess) { delete P; return cuda_fail(e, "pattern device alloc"); }
@@ -207,6 +229,11 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     D.q = blk + off[idx++];
     D.fwd_lev = blk + off[idx++];
     D.bwd_lev = blk + off[idx++];
+    D.bwd_pos = blk + off[idx++];
+    D.fwd_ldesc = blk + off[idx++];
+    D.bwd_ldesc = blk + off[idx++];
+    D.lev_max_ent = S.lev_max_ent;
+    D.lev_max_rows = S.lev_max_rows;
     D.nfwd_levels = S.nfwd_levels;
     D.nbwd_levels = S.nbwd_levels;
     D.k0 = S.k0;
@@ -264,11 +291,12 @@ static size_t smem_fixed(int nwords) { return 64 + (((size_t)nwords * 4 + 15) & 
 
 void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm, int m, int vsize,
                SmemPlan& plan) {
-    (void)vsize;
-    int nmax = 1, levmax = 1;
+    int nmax = 1, levmax = 1, entmax = 4, rowmax = 4;
     for (auto* p : pats) {
         nmax = std::max(nmax, p->S.n);
         levmax = std::max(levmax, p->S.nfwd_levels + p->S.nbwd_levels);
+        entmax = std::max(entmax, p->S.lev_max_ent);
+        rowmax = std::max(rowmax, p->S.lev_max_rows);
     }
     (void)block;
     const size_t limit = 227 * 1024;
@@ -286,9 +314,31 @@ void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm,
     // descriptors (row order, row pointers, level bounds of both sweeps)
     // when they fit beside it.
     plan.ycap = ((size_t)nmax * 8 <= avail) ? nmax : 0;
-    const size_t dneed = 4 * (size_t)nmax + (size_t)levmax + 8;
+    const size_t dneed = 4 * (size_t)nmax + (size_t)levmax + 8 + 5 * (size_t)levmax + 16;
     plan.dcap = (plan.ycap && (size_t)nmax * 8 + dneed * 4 <= avail) ? (int)dneed : 0;
-    plan.bytes = fixed + (size_t)plan.ycap * 8 + hbytes + (size_t)plan.dcap * 4;
+    // Stage ring of the level sweeps: the widest level, or as many entries
+    // as fit (at least 256; wider levels then read global memory).
+    plan.sc_ent = 0;
+    plan.sc_rows = 0;
+    if (plan.dcap) {
+        const size_t used = sweep_desc_offset(plan.ycap, m) - hbytes + (((size_t)plan.dcap + 3) & ~(size_t)3) * 4;
+        const size_t left = avail > used ? avail - used : 0;
+        int ce = (entmax + 3) & ~3, cr = (rowmax + 3) & ~3;
+        while (ce > 256 && kStages * stage_bytes(ce, cr, vsize) > left) ce = (ce / 2 + 3) & ~3;
+        while (cr > 64 && kStages * stage_bytes(ce, cr, vsize) > left) cr = (cr / 2 + 3) & ~3;
+        if (kStages * stage_bytes(ce, cr, vsize) <= left) {
+            plan.sc_ent = ce;
+            plan.sc_rows = cr;
+        }
+    }
+    plan.bytes = fixed + sweep_desc_offset(plan.ycap, m) + (((size_t)plan.dcap + 3) & ~(size_t)3) * 4 +
+                 (plan.sc_ent ? kStages * stage_bytes(plan.sc_ent, plan.sc_rows, vsize) : 0);
+}
+
+void resolve_solve_shape(lusp_batch_opts& o, int nsys) {
+    const bool few = nsys <= sm_count();
+    if (o.block_threads <= 0) o.block_threads = few ? 512 : 256;
+    if (o.ctas_per_sm <= 0) o.ctas_per_sm = few ? 1 : 2;
 }
 
 int refactor_block(const lusp_batch_opts& o, int nsys) {
@@ -330,19 +380,30 @@ void make_refactor_plan(const std::vector<PatternObj*>& pats, int threads, int v
     plan.wcap = wcap;
     plan.scap = scap;
     plan.bytes = fixed + (size_t)nw * need(wcap, scap);
-    // Dense trailing block: panel [D][nb] + U tile [nb][64] + nb column
-    // maxima, reusing the per-warp area after the sparse phase.  Widest
-    // panel (32, 16, 8) that fits the budget.
+}
+
+void make_dense_plan(const std::vector<PatternObj*>& pats, int threads, SmemPlan& plan) {
     int dmax = 0;
     for (auto* p : pats) dmax = std::max(dmax, p->S.dtail);
-    plan.tnb = 0;
-    if (dmax > 0) {
-        auto dneed = [&](int nb) { return fixed + 8 * ((size_t)dmax * nb + (size_t)nb * 64 + nb); };
-        int nb = 32;
-        while (nb > 8 && dneed(nb) > std::max(budget, plan.bytes)) nb /= 2;
-        plan.tnb = nb;
-        plan.bytes = std::max(plan.bytes, dneed(nb));
-    }
+    plan = SmemPlan{};
+    plan.nwords = 1;
+    const size_t fixed = smem_fixed(plan.nwords);
+    const size_t budget = 227 * 1024;
+    plan.bytes = fixed;
+    if (dmax == 0) return;
+    // Panel [D][nb] + U tile [nb][128] + nb column maxima + 4 cycle
+    // counters: the widest panel (32, 16, 8) that fits.
+    auto dneed = [&](int nb) { return fixed + 8 * ((size_t)dmax * nb + (size_t)nb * 128 + nb + 4); };
+    int nb = 32;
+    while (nb > 8 && dneed(nb) > budget) nb /= 2;
+    plan.tnb = nb;
+    plan.bytes = dneed(nb);
+    // The transpose reuses the area: a padded 32 x 33 fp64 tile per warp.
+    const size_t tile_b = 32 * 33 * sizeof(double);
+    int ttw = (int)std::min<size_t>({(size_t)threads / 32, 16, (budget - fixed) / tile_b});
+    ttw = std::max(1, ttw);
+    plan.ttw = ttw;
+    plan.bytes = std::max(plan.bytes, fixed + ttw * tile_b);
 }
 
 // Raise the dynamic shared-memory limit of one kernel (once per size; not a
@@ -377,6 +438,13 @@ static int refactor_prepare(size_t smem, int block, int* occ) {
     return prepare_kernel(refactor_kernel<VT>, smem, block, occ, &granted, mu);
 }
 
+template <typename VT>
+static int dense_prepare(size_t smem, int block, int* occ) {
+    static std::mutex mu;
+    static size_t granted = 0;
+    return prepare_kernel(dense_kernel<VT>, smem, block, occ, &granted, mu);
+}
+
 int refactor_occupancy(int prec, size_t smem, int block, int* occ) {
     if (prec == LUSP_FP64) return refactor_prepare<double>(smem, block, occ);
     return refactor_prepare<float>(smem, block, occ);
@@ -390,7 +458,7 @@ int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ) {
 
 template <typename VT, typename AT>
 static int launch_typed(const LaunchArgs& a, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(a.d_queue, 0, 2 * sizeof(int), st);
+    cudaError_t e = cudaMemsetAsync(a.d_queue, 0, 3 * sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "queue reset");
     if (a.what & LUSP_RUN_REFACTOR) {
         int rc = refactor_prepare<VT>(a.rplan.bytes, a.rblock, nullptr);
@@ -398,6 +466,13 @@ static int launch_typed(const LaunchArgs& a, cudaStream_t st) {
         refactor_kernel<VT><<<a.rgrid, a.rblock, a.rplan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.rplan, a.prm);
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "refactor kernel launch");
+        if (a.dgrid > 0) {
+            rc = dense_prepare<VT>(a.dplan.bytes, a.dblock, nullptr);
+            if (rc != LUSP_OK) return rc;
+            dense_kernel<VT><<<a.dgrid, a.dblock, a.dplan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.dplan, a.prm);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return cuda_fail(e, "dense kernel launch");
+        }
     }
     if (a.what & LUSP_RUN_SOLVE) {
         int rc = kernel_prepare<VT, AT>(a.plan.bytes, a.block, nullptr);
@@ -417,15 +492,15 @@ int launch_systems(const LaunchArgs& a, cudaStream_t st) {
     return launch_typed<float, float>(a, st);
 }
 
-int launch_kernel_count(int what) {
-    return ((what & LUSP_RUN_REFACTOR) ? 1 : 0) + ((what & LUSP_RUN_SOLVE) ? 1 : 0);
+int launch_kernel_count(const LaunchArgs& a, int what) {
+    return ((what & LUSP_RUN_REFACTOR) ? (a.dgrid > 0 ? 2 : 1) : 0) + ((what & LUSP_RUN_SOLVE) ? 1 : 0);
 }
 
 int batch_launch(BatchObj* B, int what, cudaStream_t st) {
     LaunchArgs a = B->launch;
     a.what = what;
     int rc = launch_systems(a, st);
-    if (rc == LUSP_OK) B->launches = launch_kernel_count(what);
+    if (rc == LUSP_OK) B->launches = launch_kernel_count(a, what);
     return rc;
 }
 
@@ -436,25 +511,24 @@ int tail_ld(const StaticPattern& S) { return (S.dtail + 31) & ~31; }
 size_t system_private_bytes(const StaticPattern& S, size_t vs, int m) {
     const size_t n = S.n;
     const size_t st = S.sell_ptr.back();
-    return al256(S.cap * vs) + al256(S.lci.size() * vs) + al256(S.uci.size() * vs) + al256(n * vs) +
-           al256(st * 8) + al256(st * 4) + al256(((size_t)m + 8) * n * 8) +
-           al256((size_t)S.dtail * tail_ld(S) * vs);
-}
-
-size_t tail_work_doubles(const std::vector<PatternObj*>& pats) {
-    size_t m = 0;
-    for (auto* p : pats) m = std::max(m, (size_t)p->S.dtail * tail_ld(p->S));
-    return (m + 31) & ~(size_t)31;
+    // The row-major values and the sweep-order diagonal get 64 bytes of
+    // slack: the sweeps copy them in aligned 16-byte pieces.
+    return al256(S.cap * vs) + al256(S.lci.size() * vs + 64) + al256(S.uci.size() * vs + 64) + al256(n * vs) +
+           al256(n * vs + 64) + al256(st * 8) + al256(st * 4) + al256(((size_t)m + 8) * n * 8) +
+           al256((size_t)S.dtail * tail_ld(S) * vs) + al256((size_t)S.dtail * tail_ld(S) * 8);
 }
 
 char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m) {
     const size_t n = S.n;
     const size_t st = S.sell_ptr.back();
     D.tail = p; p += al256((size_t)S.dtail * tail_ld(S) * vs);
+    D.tailw = S.dtail > 0 ? (double*)p : nullptr;
+    p += al256((size_t)S.dtail * tail_ld(S) * 8);
     D.lu = p; p += al256(S.cap * vs);
-    D.lval = p; p += al256(S.lci.size() * vs);
-    D.uval = p; p += al256(S.uci.size() * vs);
+    D.lval = p; p += al256(S.lci.size() * vs + 64);
+    D.uval = p; p += al256(S.uci.size() * vs + 64);
     D.udiag = p; p += al256(n * vs);
+    D.udiag_bwd = p; p += al256(n * vs + 64);
     D.sell64 = (double*)p; p += al256(st * 8);
     D.sell32 = (float*)p; p += al256(st * 4);
     D.work = (double*)p; p += al256(((size_t)m + 8) * n * 8);
@@ -468,7 +542,11 @@ size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& rplan) {
 int check_opts(const lusp_batch_opts* o) {
     if (o->prec != LUSP_MIXED && o->prec != LUSP_FP64) { set_error("bad prec"); return LUSP_EARG; }
     if (o->krylov < 1 || o->krylov > kMaxKrylov) { set_error("krylov must be 1..%d", kMaxKrylov); return LUSP_EARG; }
-    if (o->block_threads < 64 || o->block_threads > 512 || o->block_threads % 32) { set_error("block_threads must be 64..512, a multiple of 32"); return LUSP_EARG; }
+    if (o->block_threads != 0 && (o->block_threads < 64 || o->block_threads > 512 || o->block_threads % 32)) {
+        set_error("block_threads must be 0 (auto) or 64..512, a multiple of 32");
+        return LUSP_EARG;
+    }
+    if (o->ctas_per_sm < 0) { set_error("ctas_per_sm must be >= 0"); return LUSP_EARG; }
     if (o->inner_prec < 0 || o->inner_prec > 1) { set_error("bad inner_prec"); return LUSP_EARG; }
     if (o->refactor_threads != 0 &&
         (o->refactor_threads < 64 || o->refactor_threads > 1024 || o->refactor_threads % 32)) {
@@ -497,13 +575,30 @@ int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& 
     if (rc != LUSP_OK) return rc;
     if (occ < 1) { set_error("refactor kernel does not fit one SM (smem %zu)", a.rplan.bytes); return LUSP_EARG; }
     a.rgrid = std::min(nsys, occ * sm_count());
+    // Dense trailing blocks: their own kernel when any system has one.
+    int ntail = 0;
+    for (auto* p : pats) ntail += p->S.dtail > 0 ? 1 : 0;
+    a.dblock = 512;
+    a.dgrid = 0;
+    if (ntail > 0) {
+        make_dense_plan(pats, a.dblock, a.dplan);
+        int docc = 0;
+        rc = o.prec == LUSP_FP64 ? dense_prepare<double>(a.dplan.bytes, a.dblock, &docc)
+                                 : dense_prepare<float>(a.dplan.bytes, a.dblock, &docc);
+        if (rc != LUSP_OK) return rc;
+        if (docc < 1) { set_error("dense kernel does not fit one SM (smem %zu)", a.dplan.bytes); return LUSP_EARG; }
+        a.dgrid = std::min(ntail, docc * sm_count());
+    }
     return LUSP_OK;
 }
 
 int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, SmemPlan& plan) {
     make_plan(pats, o.block_threads, o.ctas_per_sm, o.krylov, o.prec == LUSP_FP64 ? 8 : 4, plan);
-    if (o.solve_sweep == 1) plan.dcap = 0;   // dataflow sweeps only
-    if (o.solve_sweep == 2 && plan.dcap == 0) {
+    if (o.solve_sweep == 1) {   // dataflow sweeps only
+        plan.dcap = 0;
+        plan.sc_ent = plan.sc_rows = 0;
+    }
+    if (o.solve_sweep == 2 && (plan.dcap == 0 || plan.sc_ent == 0)) {
         set_error("level-synchronous sweeps need the solve vector and descriptors in shared memory");
         return LUSP_EARG;
     }
@@ -517,6 +612,9 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
         if (!pats[s]) { set_error("batch_create: null pattern %d", s); return LUSP_EARG; }
     int rc = check_opts(o);
     if (rc != LUSP_OK) return rc;
+    lusp_batch_opts oo = *o;
+    resolve_solve_shape(oo, nsys);
+    o = &oo;
     BatchObj* B = new BatchObj();
     B->nsys = nsys;
     B->prec = o->prec;
@@ -550,10 +648,7 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     rc = refactor_setup(B->pats, *o, nsys, a);
     if (rc != LUSP_OK) { delete B; return rc; }
     const size_t spill = spill_bytes(a.rgrid, a.rblock, colmax, a.rplan);
-    const size_t tws = tail_work_doubles(B->pats);
-    const size_t tail_bytes = al256((size_t)a.rgrid * tws * 8);
-    const size_t total = base[nsys] + spill + tail_bytes + al256(sizeof(SysStats) * nsys) +
-                         al256(sizeof(SysDev) * nsys) + 256;
+    const size_t total = base[nsys] + spill + al256(sizeof(SysStats) * nsys) + al256(sizeof(SysDev) * nsys) + 256;
     char* blk = nullptr;
     cudaError_t e = cudaMalloc(&blk, total);
     if (e != cudaSuccess) { delete B; return cuda_fail(e, "batch device alloc"); }
@@ -561,8 +656,7 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     B->bytes = total;
     e = cudaMemset(blk, 0, total);
     if (e != cudaSuccess) { batch_free(B); return cuda_fail(e, "batch memset"); }
-    double* tail_ptr = tws ? (double*)(blk + base[nsys] + spill) : nullptr;
-    char* stats_base = blk + base[nsys] + spill + tail_bytes;
+    char* stats_base = blk + base[nsys] + spill;
     B->d_stats = (SysStats*)stats_base;
     B->d_sys = (SysDev*)(stats_base + al256(sizeof(SysStats) * nsys));
     B->d_queue = (int*)((char*)B->d_sys + al256(sizeof(SysDev) * nsys));
@@ -579,8 +673,6 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
         D.x = B->d_x + B->vec_off[s];
         carve_system(D, blk + base[s], B->pats[s]->S, vs, o->krylov);
         D.scratch = spill_ptr;
-        D.tailws = tail_ptr;
-        D.tailws_stride = (long long)tws;
         D.stats = B->d_stats + s;
     }
     e = cudaMemcpy(B->d_sys, B->h_sys.data(), sizeof(SysDev) * nsys, cudaMemcpyHostToDevice);

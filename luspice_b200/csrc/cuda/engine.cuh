@@ -46,6 +46,10 @@ struct PatternDev {
     // Dense trailing block: rows/columns [k0, n), dtail = n - k0 (0: none),
     // stored row-major with leading dimension tail_ld.
     int k0, dtail, tail_ld;
+    const int* bwd_pos;      // [n] row -> index in bwd_order
+    const int* fwd_ldesc;    // [nfwd_levels * 5] level descriptors (see host)
+    const int* bwd_ldesc;    // [nbwd_levels * 5]
+    int lev_max_ent, lev_max_rows;   // widest sweep level (entries, rows)
 };
 
 // Per-system statistics written by the kernels.
@@ -68,6 +72,8 @@ struct SysStats {
     long long cyc_lsolve, cyc_tail, cyc_usolve, cyc_spmv, cyc_solve;
     // Refactor: dense trailing block panels, U-row solves, trailing updates.
     long long cyc_tpanel, cyc_ttrsm, cyc_tupdate;
+    // Solve: dense-tail diagonal-block chains and block-column products.
+    long long cyc_tdiag, cyc_tgemv;
 };
 
 // One system: pattern + values + vectors + workspace.
@@ -78,6 +84,7 @@ struct SysDev {
     void* lval;              // [nnz_l] strict L by rows (VT)
     void* uval;              // [nnz_u] strict U by rows (VT)
     void* udiag;             // [n] U(k,k) (VT)
+    void* udiag_bwd;         // [n] U(k,k) (VT) in backward sweep order
     double* sell64;          // [sell_total] A in SELL, fp64
     float* sell32;           // [sell_total] A in SELL, fp32
     const double* b;         // [n] right-hand side, original row order
@@ -86,9 +93,10 @@ struct SysDev {
     double* scratch;         // per-CTA refactor spill (columns longer than
                              // the shared-memory work area), may be null
     void* tail;              // [dtail * tail_ld] dense L\U of the trailing
-                             // block (VT), unit L below the diagonal
-    double* tailws;          // refactor CTAs' fp64 trailing-block work areas
-    long long tailws_stride; // doubles per CTA in tailws
+                             // block (VT, column-major: (i, c) at c * ld + i),
+                             // unit L below the diagonal
+    double* tailw;           // [dtail * tail_ld] fp64 trailing block (row-major)
+                             // between the refactor and dense kernels
     SysStats* stats;
 };
 
@@ -111,6 +119,8 @@ struct SmemPlan {
     int wcap;                // per-warp refactor work slots
     int scap;                // per-warp staged L entries (refactor gathers)
     int tnb;                 // panel width of the dense trailing block
+    int ttw;                 // warps transposing the dense block (32x33 fp64 tile each)
+    int sc_ent, sc_rows;     // sweep stage capacity (entries, rows; 0: no stages)
     int ycap;                // doubles for a shared-memory solve vector
     int dcap;                // ints for shared-memory sweep descriptors
     int m;                   // Krylov dimension for H

@@ -38,6 +38,9 @@ struct LaunchArgs {
     SmemPlan rplan{};                // refactorization kernel
     int rblock = 1024;
     int rgrid = 1;
+    SmemPlan dplan{};                // dense trailing-block kernel (dgrid 0: none)
+    int dblock = 512;
+    int dgrid = 0;
 };
 
 struct GraphEntry {
@@ -88,15 +91,17 @@ int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, Sme
 int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ);
 int refactor_occupancy(int prec, size_t smem, int block, int* occ);
 int refactor_block(const lusp_batch_opts& o, int nsys);
+// Solve-kernel CTA size and plan target for nsys systems when left at 0.
+void resolve_solve_shape(lusp_batch_opts& o, int nsys);
 void make_refactor_plan(const std::vector<PatternObj*>& pats, int threads, int vsize, SmemPlan& plan);
 // Refactorization kernel block, plan and grid for nsys systems of pats.
 int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, int nsys, LaunchArgs& a);
 // Kernels one launch with these RUN_* flags issues.
-int launch_kernel_count(int what);
+int launch_kernel_count(const LaunchArgs& a, int what);
+void make_dense_plan(const std::vector<PatternObj*>& pats, int threads, SmemPlan& plan);
 size_t system_private_bytes(const StaticPattern& S, size_t vs, int m);
 int tail_ld(const StaticPattern& S);
-// fp64 trailing-block work area of one refactor CTA (doubles).
-size_t tail_work_doubles(const std::vector<PatternObj*>& pats);
+
 char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m);
 size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& rplan);
 int launch_systems(const LaunchArgs& a, cudaStream_t st);

@@ -61,6 +61,59 @@ __device__ __forceinline__ int warp_claim(int* counter) {
     return __shfl_sync(0xffffffffu, idx, 0);
 }
 
+// Pivot statistics of a CTA: warp reductions, then per-warp partials
+// combined in order by thread 0.  first: overwrite the system's statistics
+// (refactor kernel), else merge into them (dense trailing-block kernel).
+// Status bits go through sm.ctl[1], the singular column through sm.ctl[2].
+__device__ void cta_store_pivot_stats(SysStats* st, Smem& sm, double minpiv, double minratio, double maxu,
+                                      int bad, bool first) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    minpiv = warp_min(minpiv);
+    minratio = warp_min(minratio);
+    maxu = warp_max(maxu);
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    __syncthreads();
+    if (lane == 0) {
+        sm.red[warp] = minpiv;
+        atomicOr(&sm.ctl[1], bad);
+    }
+    __syncthreads();
+    double a = INFINITY;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < nw; w++) a = fmin(a, sm.red[w]);
+    __syncthreads();
+    if (lane == 0) sm.red[warp] = minratio;
+    __syncthreads();
+    double b = INFINITY;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < nw; w++) b = fmin(b, sm.red[w]);
+    __syncthreads();
+    if (lane == 0) sm.red[warp] = maxu;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double c = 0.0;
+        for (int w = 0; w < nw; w++) c = fmax(c, sm.red[w]);
+        const int sc = sm.ctl[2] == 0x7fffffff ? -1 : sm.ctl[2];
+        if (first) {
+            st->min_abs_pivot = a;
+            st->min_pivot_ratio = b;
+            st->max_abs_u = c;
+            st->status = sm.ctl[1];
+            st->singular_col = sc;
+            st->nres = 0;
+            st->inner_iters = 0;
+            st->outer_iters = 0;
+        } else {
+            st->min_abs_pivot = fmin(st->min_abs_pivot, a);
+            st->min_pivot_ratio = fmin(st->min_pivot_ratio, b);
+            st->max_abs_u = fmax(st->max_abs_u, c);
+            st->status |= sm.ctl[1];
+            if (sc >= 0 && (st->singular_col < 0 || sc < st->singular_col)) st->singular_col = sc;
+        }
+    }
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // Dense trailing block of the refactorization (rows and columns [k0, n)),
 // in place in W (fp64, row-major, leading dimension ld).  On entry W holds
@@ -76,13 +129,16 @@ template <typename VT>
 __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, const SmemPlan& plan,
                                   const SolveParams& prm, double& minpiv, double& minratio, int& bad,
                                   SysStats* st) {
-    long long c_pan = 0, c_trsm = 0, c_upd = 0, tk = clock64();
     const int D = P.dtail, ld = P.tail_ld, k0 = P.k0, nb = plan.tnb;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     double* pan = (double*)sm.uni;                                           // [D][nb]
-    double* ut = pan + (size_t)D * nb;                                       // [nb][64]
-    unsigned long long* cmax = (unsigned long long*)(ut + (size_t)nb * 64);  // [nb]
-    const int tx = tid & 63, ty = tid >> 6, nty = nt >> 6;
+    double* ut = pan + (size_t)D * nb;                                       // [nb][128]
+    unsigned long long* cmax = (unsigned long long*)(ut + (size_t)nb * 128); // [nb]
+    long long* ctr = (long long*)(cmax + nb);   // [4] stage cycles (thread 0)
+    if (tid == 0) {
+        ctr[0] = ctr[1] = ctr[2] = 0;
+        ctr[3] = clock64();
+    }
     for (int jb = 0; jb < D; jb += nb) {
         const int w = min(nb, D - jb), R = D - jb;
         for (int t = tid; t < R * nb; t += nt) {
@@ -146,10 +202,10 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
             if (c < w) W[(size_t)(jb + r) * ld + jb + c] = pan[t];
         }
         __syncthreads();
-        {
+        if (tid == 0) {
             const long long t2 = clock64();
-            c_pan += t2 - tk;
-            tk = t2;
+            ctr[0] += t2 - ctr[3];
+            ctr[3] = t2;
         }
         const int c1 = jb + w, ncols = D - c1;
         if (ncols <= 0) break;
@@ -183,56 +239,72 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
             }
         }
         __syncthreads();
-        {
+        if (tid == 0) {
             const long long t2 = clock64();
-            c_trsm += t2 - tk;
-            tk = t2;
+            ctr[1] += t2 - ctr[3];
+            ctr[3] = t2;
         }
-        // Trailing update W22 -= L21 U12, tiles of (4 * nty) rows x 64
-        // columns, four rows per thread, multipliers from the panel in
-        // shared memory and U12 staged per tile.
-        const int TR = 4 * nty;
-        const int nrt = (ncols + TR - 1) / TR, nct = (ncols + 63) / 64;
+        // Trailing update W22 -= L21 U12, tiles of (4 * nw) rows x 128
+        // columns: a thread owns four rows (one per warp stride) and four
+        // columns (lane + 32 j); multipliers from the panel in shared memory
+        // (broadcast within a warp), U12 staged per tile.
+        const int TR = 4 * nw;
+        const int nrt = (ncols + TR - 1) / TR, nct = (ncols + 127) / 128;
         for (int tile = 0; tile < nrt * nct; tile++) {
-            const int r0 = c1 + (tile / nct) * TR, q0 = c1 + (tile % nct) * 64;
-            for (int t = tid; t < w * 64; t += nt) {
-                const int c = t >> 6, x = t & 63;
+            const int r0 = c1 + (tile / nct) * TR, q0 = c1 + (tile % nct) * 128;
+            for (int t = tid; t < w * 128; t += nt) {
+                const int c = t >> 7, x = t & 127;
                 ut[t] = q0 + x < D ? W[(size_t)(jb + c) * ld + q0 + x] : 0.0;
             }
             __syncthreads();
-            const int col = q0 + tx;
-            if (col < D) {
-                double acc[4];
-                int row[4];
+            const int rw = r0 + warp;
+            if (rw < D) {
+                double acc[4][4];
+                int lo[4];
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    row[q] = r0 + ty + q * nty;
-                    acc[q] = row[q] < D ? W[(size_t)row[q] * ld + col] : 0.0;
+                    const int row = rw + q * nw;
+                    lo[q] = row < D ? q * nw * nb : 0;   // rows past the block reuse rw's multipliers
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const int col = q0 + lane + 32 * j;
+                        acc[q][j] = (row < D && col < D) ? W[(size_t)row * ld + col] : 0.0;
+                    }
                 }
+                const double* l0 = pan + (size_t)(rw - jb) * nb;
                 for (int c = 0; c < w; c++) {
-                    const double u = ut[c * 64 + tx];
+                    double u[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) u[j] = ut[c * 128 + lane + 32 * j];
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
-                        const int rr = min(row[q], D - 1) - jb;
-                        acc[q] = __dsub_rn(acc[q], __dmul_rn(pan[rr * nb + c], u));
+                        const double l = l0[lo[q] + c];
+#pragma unroll
+                        for (int j = 0; j < 4; j++) acc[q][j] = __dsub_rn(acc[q][j], __dmul_rn(l, u[j]));
                     }
                 }
 #pragma unroll
-                for (int q = 0; q < 4; q++)
-                    if (row[q] < D) W[(size_t)row[q] * ld + col] = acc[q];
+                for (int q = 0; q < 4; q++) {
+                    const int row = rw + q * nw;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const int col = q0 + lane + 32 * j;
+                        if (row < D && col < D) W[(size_t)row * ld + col] = acc[q][j];
+                    }
+                }
             }
             __syncthreads();
         }
-        {
+        if (tid == 0) {
             const long long t2 = clock64();
-            c_upd += t2 - tk;
-            tk = t2;
+            ctr[2] += t2 - ctr[3];
+            ctr[3] = t2;
         }
     }
     if (tid == 0) {
-        st->cyc_tpanel = c_pan;
-        st->cyc_ttrsm = c_trsm;
-        st->cyc_tupdate = c_upd;
+        st->cyc_tpanel = ctr[0];
+        st->cyc_ttrsm = ctr[1];
+        st->cyc_tupdate = ctr[2];
     }
 }
 
@@ -240,18 +312,35 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
 // diagonal, U on and above) and the merged / row-major slot arrays of the
 // tail columns' rows >= k0.
 template <typename VT>
-__device__ void dense_tail_store(const SysDev& S, const PatternDev& P, const double* W, double& maxu) {
+__device__ void dense_tail_store(const SysDev& S, const PatternDev& P, const double* W, double& maxu,
+                                 char* smem_tail_tiles, int ttw) {
     const int D = P.dtail, ld = P.tail_ld, k0 = P.k0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     VT* T = (VT*)S.tail;
-    for (size_t t = threadIdx.x; t < (size_t)D * ld; t += blockDim.x) {
-        const int i = (int)(t / ld), c = (int)(t - (size_t)i * ld);
-        if (c < D) {
-            const double v = W[t];
-            if (i <= c) maxu = fmax(maxu, fabs(v));
-            T[t] = ValTraits<VT>::to(v);
-        } else {
-            T[t] = ValTraits<VT>::to(0.0);
+    // T is column-major (element (i, c) at T[c * ld + i]) so the solves'
+    // block-column products read consecutive rows per warp.  Transpose in
+    // 32 x 32 tiles through shared memory (a warp per tile, ttw warps,
+    // each with a padded 32 x 33 fp64 tile).
+    {
+        double* tile = (double*)smem_tail_tiles + (size_t)warp * 32 * 33;
+        const int nt32 = ld / 32, twarps = min(nw, ttw);
+        if (warp < twarps) {
+            for (int tt = warp; tt < nt32 * nt32; tt += twarps) {
+                const int ti = tt / nt32, tc = tt - ti * nt32;
+                for (int r = 0; r < 32; r++) {
+                    const int i = ti * 32 + r, c = tc * 32 + lane;
+                    double v = 0.0;
+                    if (i < D && c < D) {
+                        v = W[(size_t)i * ld + c];
+                        if (i <= c) maxu = fmax(maxu, fabs(v));
+                    }
+                    tile[r * 33 + lane] = v;
+                }
+                __syncwarp();
+                for (int c = 0; c < 32 && tc * 32 + c < D; c++)
+                    T[(size_t)(tc * 32 + c) * ld + ti * 32 + lane] = ValTraits<VT>::to(tile[lane * 33 + c]);
+                __syncwarp();
+            }
         }
     }
     __syncthreads();
@@ -267,14 +356,32 @@ __device__ void dense_tail_store(const SysDev& S, const PatternDev& P, const dou
         for (int t = lane; t < d; t += 32) below += rows[t] < k0;
         below = __reduce_add_sync(0xffffffffu, below);
         for (int t = below + lane; t < len; t += 32) {
-            const VT sv = T[(size_t)(rows[t] - k0) * ld + kk];
+            const VT sv = T[(size_t)kk * ld + (rows[t] - k0)];
             lu[c0 + t] = sv;
-            const int dst = P.slot_dst[c0 + t];
-            if (t < d) uval[dst] = sv;
-            else if (t == d) udiag[k] = sv;
-            else lval[dst] = sv;
+            if (t == d) udiag[k] = sv;
+            // Other slots of the block live only in the dense copy.
         }
     }
+}
+
+// The dense trailing block of one system (its own kernel: few warps, many
+// registers each): factor, store, merge the pivot statistics.
+template <typename VT>
+__device__ void dense_phase(const SysDev& S, const SmemPlan& plan, char* smem_base, const SolveParams& prm) {
+    const PatternDev& P = *S.pat;
+    if (P.dtail <= 0) return;
+    Smem sm(smem_base, plan);
+    if (threadIdx.x == 0) {
+        sm.ctl[1] = 0;
+        sm.ctl[2] = 0x7fffffff;
+    }
+    __syncthreads();
+    double minpiv = INFINITY, minratio = INFINITY, maxu = 0.0;
+    int bad = 0;
+    dense_tail_factor<VT>(P, S.tailw, sm, plan, prm, minpiv, minratio, bad, S.stats);
+    __syncthreads();
+    dense_tail_store<VT>(S, P, S.tailw, maxu, sm.uni, plan.ttw);
+    cta_store_pivot_stats(S.stats, sm, minpiv, minratio, maxu, bad, false);
 }
 
 // ---------------------------------------------------------------------------
@@ -329,7 +436,7 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
     }
     // This CTA's dense trailing block, zeroed: the tail columns scatter only
     // their pattern's entries into it.
-    double* W = P.dtail > 0 ? S.tailws + (size_t)blockIdx.x * S.tailws_stride : nullptr;
+    double* W = P.dtail > 0 ? S.tailw : nullptr;
     if (W)
         for (size_t t = threadIdx.x; t < (size_t)P.dtail * P.tail_ld; t += blockDim.x) W[t] = 0.0;
     __syncthreads();
@@ -541,64 +648,23 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
             lu[slot] = sv;
             const int dst = P.slot_dst[slot];
             if (t < d) uval[dst] = sv;
-            else if (t == d) udiag[k] = sv;
-            else lval[dst] = sv;
+            else if (t == d) {
+                udiag[k] = sv;
+                ((VT*)S.udiag_bwd)[P.bwd_pos[k]] = ValTraits<VT>::to(1.0 / piv);
+            } else lval[dst] = sv;
         }
         __threadfence_block();
         __syncwarp();
         if (lane == 0) set_ready(sm.ready, k);
     }
 
-    if (W) {
-        __syncthreads();
-        dense_tail_factor<VT>(P, W, sm, plan, prm, minpiv, minratio, bad, S.stats);
-        __syncthreads();
-        dense_tail_store<VT>(S, P, W, maxu);
-    }
     if (lane == 0) {
         atomicAdd((unsigned long long*)&S.stats->cyc_wait, (unsigned long long)c_wait);
         atomicAdd((unsigned long long*)&S.stats->cyc_gather, (unsigned long long)c_gather);
         atomicAdd((unsigned long long*)&S.stats->cyc_update, (unsigned long long)c_update);
     }
     if (threadIdx.x == 0) S.stats->cyc_refactor = clock64() - t_begin;
-    // Statistics: warp reductions, then per-warp partials combined in order.
-    minpiv = warp_min(minpiv);
-    minratio = warp_min(minratio);
-    maxu = warp_max(maxu);
-    bad = __reduce_or_sync(0xffffffffu, bad);
-    __syncthreads();
-    if (lane == 0) {
-        sm.red[warp] = minpiv;
-        atomicOr(&sm.ctl[1], bad);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = INFINITY;
-        for (int w = 0; w < nw; w++) a = fmin(a, sm.red[w]);
-        S.stats->min_abs_pivot = a;
-    }
-    __syncthreads();
-    if (lane == 0) sm.red[warp] = minratio;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = INFINITY;
-        for (int w = 0; w < nw; w++) a = fmin(a, sm.red[w]);
-        S.stats->min_pivot_ratio = a;
-    }
-    __syncthreads();
-    if (lane == 0) sm.red[warp] = maxu;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0.0;
-        for (int w = 0; w < nw; w++) a = fmax(a, sm.red[w]);
-        S.stats->max_abs_u = a;
-        S.stats->status = sm.ctl[1];
-        S.stats->singular_col = sm.ctl[2] == 0x7fffffff ? -1 : sm.ctl[2];
-        S.stats->nres = 0;
-        S.stats->inner_iters = 0;
-        S.stats->outer_iters = 0;
-    }
-    __syncthreads();
+    cta_store_pivot_stats(S.stats, sm, minpiv, minratio, maxu, bad, true);
 }
 
 // ---------------------------------------------------------------------------
@@ -607,13 +673,13 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
 // warp through shuffles, the rest of the block's columns as one
 // multiply-add per row and thread.  fp64 accumulation.
 // ---------------------------------------------------------------------------
-// sum_{c < w} row[c] * y[c] for one 32-column block of a tail row: all
-// loads issued before the multiply-adds.
+// sum_{c < w} row[c * stride] * y[c] for one 32-column block of a tail row
+// (column-major factor): all loads issued before the multiply-adds.
 template <typename VT>
-__device__ __forceinline__ double tail_row_dot(const VT* row, const double* y, int w) {
+__device__ __forceinline__ double tail_row_dot(const VT* row, size_t stride, const double* y, int w) {
     VT v[32];
 #pragma unroll
-    for (int c = 0; c < 32; c++) v[c] = c < w ? row[c] : VT(0);
+    for (int c = 0; c < 32; c++) v[c] = c < w ? row[c * stride] : VT(0);
     double acc = 0.0;
 #pragma unroll
     for (int c = 0; c < 32; c++)
@@ -621,45 +687,23 @@ __device__ __forceinline__ double tail_row_dot(const VT* row, const double* y, i
     return acc;
 }
 
-// y[k0..n) := L_tt^-1 (y - L_ts y_s): first the tail rows' entries in the
-// columns before k0, then the unit-lower dense solve.
+// y[k0..n) := L_tt^-1 y[k0..n) (unit lower; the tail rows' entries in the
+// columns before k0 were applied by the forward sweep's last level).
 template <typename VT>
-__device__ void tail_forward(const PatternDev& P, const VT* lval, const VT* T, double* y) {
-    const int n = P.n, k0 = P.k0, D = P.dtail, ld = P.tail_ld;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int i = k0 + warp; i < n; i += nw) {
-        // Tail rows sit at sweep index i; their entries ascend by column.
-        const int p0 = P.lrp[i], p1 = P.lrp[i + 1];
-        double acc = 0.0;
-        int p = p0 + lane;
-        for (; p + 96 < p1; p += 128) {
-            int jj[4];
-            double vv[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                jj[q] = P.lci[p + 32 * q];
-                vv[q] = ValTraits<VT>::load(lval + p + 32 * q);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (jj[q] < k0) acc = fma(vv[q], y[jj[q]], acc);
-        }
-        for (; p < p1; p += 32) {
-            const int j = P.lci[p];
-            if (j < k0) acc = fma(ValTraits<VT>::load(lval + p), y[j], acc);
-        }
-        acc = warp_sum(acc);
-        if (lane == 0) y[i] -= acc;
-    }
-    __syncthreads();
+__device__ void tail_forward(const PatternDev& P, const VT* T, double* y, SysStats* st) {
+    const int k0 = P.k0, D = P.dtail, ld = P.tail_ld;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long c_diag = 0, c_gemv = 0;
     double* yt = y + k0;
     for (int jb = 0; jb < D; jb += 32) {
         const int w = min(32, D - jb);
+        const long long ta = clock64();
         if (warp == 0) {
             double lr[32];
-            const VT* row = T + (size_t)(jb + lane) * ld + jb;
+            const VT* row = T + (size_t)jb * ld + jb + lane;
 #pragma unroll
-            for (int c = 0; c < 32; c++) lr[c] = (c < lane && lane < w) ? ValTraits<VT>::load(row + c) : 0.0;
+            for (int c = 0; c < 32; c++)
+                lr[c] = (c < lane && lane < w) ? ValTraits<VT>::load(row + (size_t)c * ld) : 0.0;
             double yr = lane < w ? yt[jb + lane] : 0.0;
 #pragma unroll
             for (int c = 0; c < 31; c++) {
@@ -669,26 +713,37 @@ __device__ void tail_forward(const PatternDev& P, const VT* lval, const VT* T, d
             if (lane < w) yt[jb + lane] = yr;
         }
         __syncthreads();
+        const long long tb = clock64();
         for (int i = jb + w + threadIdx.x; i < D; i += blockDim.x)
-            yt[i] -= tail_row_dot<VT>(T + (size_t)i * ld + jb, yt + jb, w);
+            yt[i] -= tail_row_dot<VT>(T + (size_t)jb * ld + i, ld, yt + jb, w);
         __syncthreads();
+        const long long tc = clock64();
+        c_diag += tb - ta;
+        c_gemv += tc - tb;
+    }
+    if (threadIdx.x == 0) {
+        st->cyc_tdiag += c_diag;
+        st->cyc_tgemv += c_gemv;
     }
 }
 
 // y[k0..n) := U_tt^-1 y[k0..n) (upper with diagonal).
 template <typename VT>
-__device__ void tail_backward(const PatternDev& P, const VT* T, double* y) {
+__device__ void tail_backward(const PatternDev& P, const VT* T, double* y, SysStats* st) {
     const int k0 = P.k0, D = P.dtail, ld = P.tail_ld;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long c_diag = 0, c_gemv = 0;
     double* yt = y + k0;
     for (int jb = ((D - 1) / 32) * 32; jb >= 0; jb -= 32) {
         const int w = min(32, D - jb);
+        const long long ta = clock64();
         if (warp == 0) {
             double ur[32];
-            const VT* row = T + (size_t)(jb + lane) * ld + jb;
+            const VT* row = T + (size_t)jb * ld + jb + lane;
 #pragma unroll
-            for (int c = 0; c < 32; c++) ur[c] = (c > lane && c < w) ? ValTraits<VT>::load(row + c) : 0.0;
-            const double dg = lane < w ? ValTraits<VT>::load(row + lane) : 1.0;
+            for (int c = 0; c < 32; c++)
+                ur[c] = (c > lane && c < w) ? ValTraits<VT>::load(row + (size_t)c * ld) : 0.0;
+            const double dg = lane < w ? ValTraits<VT>::load(row + (size_t)lane * ld) : 1.0;
             double yr = lane < w ? yt[jb + lane] : 0.0;
 #pragma unroll
             for (int c = 31; c >= 0; c--) {
@@ -701,9 +756,17 @@ __device__ void tail_backward(const PatternDev& P, const VT* T, double* y) {
             if (lane < w) yt[jb + lane] = yr;
         }
         __syncthreads();
+        const long long tb = clock64();
         for (int i = threadIdx.x; i < jb; i += blockDim.x)
-            yt[i] -= tail_row_dot<VT>(T + (size_t)i * ld + jb, yt + jb, w);
+            yt[i] -= tail_row_dot<VT>(T + (size_t)jb * ld + i, ld, yt + jb, w);
         __syncthreads();
+        const long long tc = clock64();
+        c_diag += tb - ta;
+        c_gemv += tc - tb;
+    }
+    if (threadIdx.x == 0) {
+        st->cyc_tdiag += c_diag;
+        st->cyc_tgemv += c_gemv;
     }
 }
 
@@ -729,7 +792,7 @@ __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval
     volatile double* vy = y;
     while (true) {
         const int idx = warp_claim(&sm.ctl[0]);
-        if (idx >= k0) break;
+        if (idx >= n) break;
         const int i = P.fwd_order[idx];
         const int p0 = P.lrp[idx], p1 = P.lrp[idx + 1];
         double acc = 0.0;
@@ -750,8 +813,8 @@ __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval
     __syncthreads();
     const long long t1 = clock64();
     if (P.dtail > 0) {
-        tail_forward<VT>(P, lval, tail, y);
-        tail_backward<VT>(P, tail, y);
+        tail_forward<VT>(P, tail, y, st);
+        tail_backward<VT>(P, tail, y, st);
     }
     const long long t2 = clock64();
     // Rows of the dense tail are complete before the sparse U sweep starts.
@@ -792,100 +855,162 @@ __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval
     }
 }
 
-// One triangular sweep, level-synchronous: the rows of a level are spread
-// over the warps (one warp per row, lanes over the row's entries), one
-// barrier per level.  Row order, row pointers and level bounds come from
-// shared memory; each warp keeps the first 32 entries (one per lane) of its
-// next two rows in registers (sets A and B, used alternately so a pending
-// load is never copied), loaded while earlier rows and barriers complete.
-// UPPER: y[i] = (y[i] - sum) / diag[i] (U sweep), else y[i] -= sum.
-template <typename VT, bool UPPER>
-__device__ void level_sweep(int nlev, const int* lev, const int* order, const int* rp,
-                            const int* ci, const VT* val, const VT* diag, double* y) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    int gl = 0, gidx = warp;
-    while (gl < nlev && gidx >= lev[gl + 1]) {
-        gl++;
-        if (gl < nlev) gidx = lev[gl] + warp;
-    }
-    int a_idx = -1, a_lvl = nlev, a_col = -1, b_idx = -1, b_lvl = nlev, b_col = -1;
-    double a_v = 0.0, a_d = 1.0, b_v = 0.0, b_d = 1.0;
-#define LUSP_FETCH(IDX, LVL, COL, V, D)                                            \
-    if (gl < nlev) {                                                              \
-        IDX = gidx;                                                               \
-        LVL = gl;                                                                 \
-        const int pp = rp[gidx] + lane;                                           \
-        COL = -1;                                                                 \
-        V = 0.0;                                                                  \
-        if (pp < rp[gidx + 1]) {                                                  \
-            COL = ci[pp];                                                         \
-            V = ValTraits<VT>::load(val + pp);                                    \
-        }                                                                         \
-        if (UPPER) D = ValTraits<VT>::load(diag + order[gidx]);                   \
-        gidx += nw;                                                               \
-        while (gl < nlev && gidx >= lev[gl + 1]) {                                \
-            gl++;                                                                 \
-            if (gl < nlev) gidx = lev[gl] + warp;                                 \
-        }                                                                         \
-    } else {                                                                      \
-        IDX = -1;                                                                 \
-        LVL = nlev;                                                               \
-    }
-#define LUSP_ROW(IDX, COL, V, D)                                                   \
-    {                                                                             \
-        const int i = order[IDX];                                                 \
-        const int p1 = rp[IDX + 1];                                               \
-        double acc = COL >= 0 ? V * y[COL] : 0.0;                                 \
-        int p = rp[IDX] + 32 + lane;                                              \
-        for (; p + 96 < p1; p += 128) {                                           \
-            int cc[4];                                                            \
-            double vv[4];                                                         \
-            _Pragma("unroll") for (int q = 0; q < 4; q++) {                       \
-                cc[q] = ci[p + 32 * q];                                           \
-                vv[q] = ValTraits<VT>::load(val + p + 32 * q);                    \
-            }                                                                     \
-            _Pragma("unroll") for (int q = 0; q < 4; q++) acc = fma(vv[q], y[cc[q]], acc); \
-        }                                                                         \
-        for (; p < p1; p += 32) acc = fma(ValTraits<VT>::load(val + p), y[ci[p]], acc); \
-        acc = warp_sum(acc);                                                      \
-        if (lane == 0) y[i] = UPPER ? (y[i] - acc) / D : y[i] - acc;              \
-    }
-    LUSP_FETCH(a_idx, a_lvl, a_col, a_v, a_d)
-    LUSP_FETCH(b_idx, b_lvl, b_col, b_v, b_d)
-    int passed = 0;   // barriers passed = levels known complete
-    while (true) {
-        if (a_idx < 0) break;
-        while (passed < a_lvl) { __syncthreads(); passed++; }
-        LUSP_ROW(a_idx, a_col, a_v, a_d)
-        LUSP_FETCH(a_idx, a_lvl, a_col, a_v, a_d)
-        if (b_idx < 0) break;
-        while (passed < b_lvl) { __syncthreads(); passed++; }
-        LUSP_ROW(b_idx, b_col, b_v, b_d)
-        LUSP_FETCH(b_idx, b_lvl, b_col, b_v, b_d)
-    }
-    while (passed < nlev) { __syncthreads(); passed++; }
-#undef LUSP_FETCH
-#undef LUSP_ROW
+// cp.async group control (sm_80+).
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// One triangular sweep, level-synchronous (one barrier per level).  Each
+// level's entries (column positions, values and, for U, the diagonal of its
+// rows in sweep order) are copied by cp.async into a ring of kStages
+// shared-memory stages, kStages - 1 levels ahead of the level being
+// computed, so a level's work reads shared memory only.  A level's rows are
+// spread over groups of g lanes, g the power of two at or above its mean
+// row length (1..32): wide levels of short rows run a row per thread,
+// narrow levels of long rows a row per warp.  Levels larger than a stage
+// read global memory directly.
+// UPPER: y[i] = (y[i] - sum) / diag (U sweep), else y[i] -= sum.
+constexpr int kStages = 4;
+
+__host__ __device__ inline size_t stage_bytes(int cap_e, int cap_r, int vsize) {
+    return (size_t)(cap_e + 8) * (4 + vsize) + (size_t)(cap_r + 8) * vsize;
 }
 
-// Shared-memory sweep descriptors of one system: [fwd_order n][fwd rp n+1]
-// [fwd_lev nfl+1][bwd_order n][bwd rp n+1][bwd_lev nbl+1].
+// The sweeps run on the first kSweepThreads threads (named barrier 1); the
+// other warps of the CTA, if any, wait at the closing CTA barrier.
+constexpr int kSweepThreads = 1024;
+
+__device__ __forceinline__ void sweep_barrier(int nthreads) {
+    asm volatile("bar.sync 1, %0;\n" ::"r"(nthreads) : "memory");
+}
+
+template <typename VT, bool UPPER>
+__device__ void staged_sweep(int nlev, const int4* ld4, const int* lgl, const int* order, const int* rp,
+                             const int* ci, const VT* val, const VT* dgo, double* y,
+                             char* stage, int cap_e, int cap_r) {
+    const int NT = min((int)blockDim.x, kSweepThreads);
+    if ((int)threadIdx.x >= NT) {
+        __syncthreads();
+        return;
+    }
+    const int CE = cap_e + 8;
+    const size_t sb = stage_bytes(cap_e, cap_r, sizeof(VT));
+    const int warp = threadIdx.x >> 5;
+    const bool pow2 = (NT & (NT - 1)) == 0;
+    const int lgb = 31 - __clz(NT);
+    auto issue = [&](int L) {
+        if (L < nlev) {
+            const int4 d = ld4[L];
+            if (d.w - d.z <= cap_e && d.y - d.x <= cap_r) {
+                char* base = stage + (size_t)(L % kStages) * sb;
+                int* sc = (int*)base;
+                VT* sv = (VT*)(base + (size_t)CE * 4);
+                VT* sd = (VT*)(base + (size_t)CE * (4 + sizeof(VT)));
+                const int a0 = d.z & ~3, n4 = ((d.w + 3) & ~3) - a0;
+                for (int t = threadIdx.x * 4; t < n4; t += NT * 4) {
+                    cp_async_16(sc + t, ci + a0 + t);
+                    cp_async_16(sv + t, val + a0 + t);
+                    if (sizeof(VT) == 8) cp_async_16(sv + t + 2, val + a0 + t + 2);
+                }
+                if (UPPER) {
+                    const int b0 = d.x & ~3, m4 = ((d.y + 3) & ~3) - b0;
+                    for (int t = threadIdx.x * 4; t < m4; t += NT * 4) {
+                        cp_async_16(sd + t, dgo + b0 + t);
+                        if (sizeof(VT) == 8) cp_async_16(sd + t + 2, dgo + b0 + t + 2);
+                    }
+                }
+            }
+        }
+        cp_async_commit();
+    };
+    for (int L = 0; L < kStages - 1; L++) issue(L);
+    for (int L = 0; L < nlev; L++) {
+        cp_async_wait_group<kStages - 2>();
+        sweep_barrier(NT);
+        issue(L + kStages - 1);
+        const int4 d = ld4[L];
+        const int r0 = d.x, r1 = d.y, nr = r1 - r0;
+        const bool st = d.w - d.z <= cap_e && nr <= cap_r;
+        char* base = stage + (size_t)(L % kStages) * sb;
+        const int* cc = st ? (const int*)base : ci;
+        const VT* vv = st ? (const VT*)(base + (size_t)CE * 4) : val;
+        const VT* dd = st ? (const VT*)(base + (size_t)CE * (4 + sizeof(VT))) : dgo;
+        const int eb = st ? (d.z & ~3) : 0, rb = st ? (r0 & ~3) : 0;
+        const int lg = lgl[L], g = 1 << lg;
+        const int lig = threadIdx.x & (g - 1);
+        const int ngr = NT >> lg;
+        const int rounds = pow2 ? (nr + ngr - 1) >> (lgb - lg) : (nr + ngr - 1) / ngr;
+        for (int rd = 0; rd < rounds; rd++) {
+            const int rbase = r0 + rd * ngr;
+            if (rbase + ((warp * 32) >> lg) >= r1) break;   // nothing left for this warp
+            const int r = rbase + ((int)threadIdx.x >> lg);
+            double acc = 0.0;
+            if (r < r1) {
+                const int pe = rp[r + 1] - eb;
+                for (int e = rp[r] - eb + lig; e < pe; e += g)
+                    acc = fma(ValTraits<VT>::load(vv + e), y[cc[e]], acc);
+            }
+            for (int o = g >> 1; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, g);
+            if (r < r1 && lig == 0) {
+                const int i = order[r];
+                if (UPPER) y[i] = (y[i] - acc) * ValTraits<VT>::load(dd + (r - rb));
+                else y[i] = y[i] - acc;
+            }
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+}
+
+// Shared-memory sweep descriptors of one system: [fwd level descriptors
+// nfl x int4][bwd level descriptors nbl x int4][fwd lanes nfl][bwd lanes
+// nbl][fwd_order n][fwd rp n+1][bwd_order n][bwd rp n+1].
 __device__ __forceinline__ bool sweep_desc_fits(const PatternDev& P, const SmemPlan& plan) {
-    return P.n <= plan.ycap && 4 * P.n + P.nfwd_levels + P.nbwd_levels + 4 <= plan.dcap;
+    return P.n <= plan.ycap && 4 * P.n + 5 * (P.nfwd_levels + P.nbwd_levels) + 4 <= plan.dcap && plan.sc_ent > 0;
+}
+
+// Byte offset (16-byte aligned) of the sweep descriptors in the solve
+// area: after the solve vector (ycap doubles) and the Hessenberg block.
+__host__ __device__ inline size_t sweep_desc_offset(int ycap, int m) {
+    const size_t b = ((size_t)ycap + (size_t)(m + 1) * m + 6 * (size_t)(m + 1)) * sizeof(double);
+    return (b + 15) & ~(size_t)15;
 }
 
 __device__ __forceinline__ int* sweep_desc_base(const SmemPlan& plan, Smem& sm) {
-    return (int*)((double*)sm.uni + plan.ycap + (size_t)(plan.m + 1) * plan.m + 6 * (size_t)(plan.m + 1));
+    return (int*)(sm.uni + sweep_desc_offset(plan.ycap, plan.m));
 }
+
+struct SweepDesc {
+    const int4 *f_ld, *b_ld;
+    const int *f_lg, *b_lg, *f_ord, *f_rp, *b_ord, *b_rp;
+    __device__ SweepDesc(const PatternDev& P, const int* d) {
+        const int n = P.n, nfl = P.nfwd_levels, nbl = P.nbwd_levels;
+        f_ld = (const int4*)d;
+        b_ld = f_ld + nfl;
+        f_lg = (const int*)(b_ld + nbl);
+        b_lg = f_lg + nfl;
+        f_ord = b_lg + nbl;
+        f_rp = f_ord + n;
+        b_ord = f_rp + n + 1;
+        b_rp = b_ord + n;
+    }
+};
 
 __device__ void load_sweep_desc(const PatternDev& P, int* d) {
     const int n = P.n, nfl = P.nfwd_levels, nbl = P.nbwd_levels;
-    int* f_ord = d;
-    int* f_rp = f_ord + n;
-    int* f_lev = f_rp + n + 1;
-    int* b_ord = f_lev + nfl + 1;
-    int* b_rp = b_ord + n;
-    int* b_lev = b_rp + n + 1;
+    const SweepDesc sd(P, d);
+    int* f_ld = (int*)sd.f_ld;
+    int* b_ld = (int*)sd.b_ld;
+    int* f_lg = (int*)sd.f_lg;
+    int* b_lg = (int*)sd.b_lg;
+    int* f_ord = (int*)sd.f_ord;
+    int* f_rp = (int*)sd.f_rp;
+    int* b_ord = (int*)sd.b_ord;
+    int* b_rp = (int*)sd.b_rp;
+    for (int t = threadIdx.x; t < 4 * nfl; t += blockDim.x) f_ld[t] = P.fwd_ldesc[t];
+    for (int t = threadIdx.x; t < 4 * nbl; t += blockDim.x) b_ld[t] = P.bwd_ldesc[t];
+    for (int t = threadIdx.x; t < nfl; t += blockDim.x) f_lg[t] = P.fwd_ldesc[4 * nfl + t];
+    for (int t = threadIdx.x; t < nbl; t += blockDim.x) b_lg[t] = P.bwd_ldesc[4 * nbl + t];
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
         f_ord[t] = P.fwd_order[t];
         b_ord[t] = P.bwd_order[t];
@@ -894,51 +1019,49 @@ __device__ void load_sweep_desc(const PatternDev& P, int* d) {
         f_rp[t] = P.lrp[t];
         b_rp[t] = P.urp[t];
     }
-    for (int t = threadIdx.x; t <= nfl; t += blockDim.x) f_lev[t] = P.fwd_lev[t];
-    for (int t = threadIdx.x; t <= nbl; t += blockDim.x) b_lev[t] = P.bwd_lev[t];
+}
+
+// Stage ring of the level-synchronous sweeps, after the descriptors.
+__device__ __forceinline__ char* sweep_stage_base(const SmemPlan& plan, Smem& sm) {
+    return (char*)(sweep_desc_base(plan, sm) + ((plan.dcap + 3) & ~3));
 }
 
 // y := U^-1 L^-1 rhs with the level-synchronous sweeps (descriptors already
-// in shared memory at d).
+// in shared memory at d, stage ring at stage).
 template <typename VT>
-__device__ void cta_lu_apply_levels(const PatternDev& P, const VT* lval, const VT* uval,
-                                    const VT* udiag, const VT* tail, const double* rhs, double* y,
-                                    const int* d, SysStats* st) {
-    const int n = P.n, nfl = P.nfwd_levels, nbl = P.nbwd_levels;
-    const int* f_ord = d;
-    const int* f_rp = f_ord + n;
-    const int* f_lev = f_rp + n + 1;
-    const int* b_ord = f_lev + nfl + 1;
-    const int* b_rp = b_ord + n;
-    const int* b_lev = b_rp + n + 1;
+__device__ void cta_lu_apply_levels(const SysDev& S, const PatternDev& P, const SmemPlan& plan,
+                                    const double* rhs, double* y, const int* d, char* stage) {
+    const int n = P.n;
+    const SweepDesc sd(P, d);
     for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = rhs[i];
     __syncthreads();
     const long long t0 = clock64();
-    level_sweep<VT, false>(nfl, f_lev, f_ord, f_rp, P.lci, lval, udiag, y);
-    __syncthreads();
+    staged_sweep<VT, false>(P.nfwd_levels, sd.f_ld, sd.f_lg, sd.f_ord, sd.f_rp, P.lci, (const VT*)S.lval,
+                            nullptr, y, stage, plan.sc_ent, plan.sc_rows);
     const long long t1 = clock64();
     if (P.dtail > 0) {
-        tail_forward<VT>(P, lval, tail, y);
-        tail_backward<VT>(P, tail, y);
+        tail_forward<VT>(P, (const VT*)S.tail, y, S.stats);
+        tail_backward<VT>(P, (const VT*)S.tail, y, S.stats);
     }
     const long long t2 = clock64();
-    level_sweep<VT, true>(nbl, b_lev, b_ord, b_rp, P.uci, uval, udiag, y);
-    __syncthreads();
-    if (threadIdx.x == 0 && st) {
-        st->cyc_lsolve += t1 - t0;
-        st->cyc_tail += t2 - t1;
-        st->cyc_usolve += clock64() - t2;
+    staged_sweep<VT, true>(P.nbwd_levels, sd.b_ld, sd.b_lg, sd.b_ord, sd.b_rp, P.uci, (const VT*)S.uval,
+                           (const VT*)S.udiag_bwd, y, stage, plan.sc_ent, plan.sc_rows);
+    if (threadIdx.x == 0) {
+        S.stats->cyc_lsolve += t1 - t0;
+        S.stats->cyc_tail += t2 - t1;
+        S.stats->cyc_usolve += clock64() - t2;
     }
 }
 
 // Dispatch: level-synchronous sweeps when their descriptors sit in shared
 // memory (desc != nullptr), else the dataflow version.
 template <typename VT>
-__device__ __forceinline__ void lu_apply(const PatternDev& P, const VT* lval, const VT* uval,
-                                         const VT* udiag, const VT* tail, const double* rhs, double* y,
-                                         Smem& sm, const int* desc, int& bad, SysStats* st) {
-    if (desc) cta_lu_apply_levels<VT>(P, lval, uval, udiag, tail, rhs, y, desc, st);
-    else cta_lu_apply<VT>(P, lval, uval, udiag, tail, rhs, y, sm, bad, st);
+__device__ __forceinline__ void lu_apply(const SysDev& S, const SmemPlan& plan, const double* rhs,
+                                         double* y, Smem& sm, const int* desc, int& bad) {
+    const PatternDev& P = *S.pat;
+    if (desc) cta_lu_apply_levels<VT>(S, P, plan, rhs, y, desc, sweep_stage_base(plan, sm));
+    else cta_lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, (const VT*)S.tail, rhs,
+                          y, sm, bad, S.stats);
 }
 
 // out = A x (RESID: out = bt - A x) with A in SELL-C-sigma, C = 32, values AT.
@@ -988,7 +1111,7 @@ __device__ void direct_phase(const SysDev& S, const SmemPlan& plan, char* smem_b
         desc = d;
     }
     const double nb = sqrt(cta_dot(bt, bt, n, sm));
-    lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, (const VT*)S.tail, bt, y, sm, desc, bad, S.stats);
+    lu_apply<VT>(S, plan, bt, y, sm, desc, bad);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         xt[i] = y[i];
         S.x[P.q[i]] = y[i];
@@ -1119,7 +1242,7 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         int jj = 0;
         for (int j = 0; j < m; j++) {
             const double* vj = V + (size_t)j * n;
-            lu_apply<VT>(P, lval, uval, udiag, tail, vj, y, sm, desc, bad, S.stats);
+            lu_apply<VT>(S, plan, vj, y, sm, desc, bad);
             const long long tsp = clock64();
             cta_spmv<AT, false>(P, ainner, y, nullptr, w);
             __syncthreads();
@@ -1190,7 +1313,7 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
             z[e] = acc;
         }
         __syncthreads();
-        lu_apply<VT>(P, lval, uval, udiag, tail, z, y, sm, desc, bad, S.stats);
+        lu_apply<VT>(S, plan, z, y, sm, desc, bad);
         double sy = 0.0, sx = 0.0;
         for (int e = threadIdx.x; e < n; e += blockDim.x) {
             xprev[e] = xt[e];

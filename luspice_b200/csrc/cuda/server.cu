@@ -282,9 +282,12 @@ bool ServerObj::try_launch(Flight& f) {
     SmemPlan plan;
     LaunchArgs la;
     int grid = 0;
-    size_t nval = 0, nvec = 0, spill = 0, tws = 0, tail_bytes = 0;
+    size_t nval = 0, nvec = 0, spill = 0;
+    const lusp_batch_opts o_req = o;
     while (true) {
         const int nsp = (int)pick.size();
+        o = o_req;
+        resolve_solve_shape(o, nsp);
         nval = nvec = 0;
         size_t privs = 0;
         int cm = 0;
@@ -304,10 +307,7 @@ bool ServerObj::try_launch(Flight& f) {
         grid = std::min(nsp, occ * sm_count());
         if (refactor_setup(pats, o, nsp, la) != LUSP_OK) return false;
         spill = spill_bytes(la.rgrid, la.rblock, cm, la.rplan);
-        tws = tail_work_doubles(pats);
-        tail_bytes = al((size_t)la.rgrid * tws * 8);
-        const size_t total = al(nval * 8) + 2 * al(nvec * 8) + privs + spill + tail_bytes +
-                             al(sizeof(SysStats) * nsp) +
+        const size_t total = al(nval * 8) + 2 * al(nvec * 8) + privs + spill + al(sizeof(SysStats) * nsp) +
                              al(sizeof(SysDev) * nsp) + 256;
         if (total <= f.arena_bytes) break;
         if (nsp == 1) {
@@ -327,8 +327,7 @@ bool ServerObj::try_launch(Flight& f) {
         pats.pop_back();
     }
     const int ns = (int)pick.size();
-    // Arena layout: values | rhs | x | per-system private | spill | tail work | stats |
-    // descriptors | queue.
+    // Arena layout: values | rhs | x | per-system private | spill | stats | descriptors | queue.
     char* a = f.arena;
     double* d_vals = (double*)a;
     double* d_rhs = (double*)(a + al(nval * 8));
@@ -351,8 +350,6 @@ bool ServerObj::try_launch(Flight& f) {
     }
     double* d_spill = spill ? (double*)p : nullptr;
     p += spill;
-    double* d_tailws = tws ? (double*)p : nullptr;
-    p += tail_bytes;
     SysStats* d_stats = (SysStats*)p;
     p += al(sizeof(SysStats) * ns);
     SysDev* d_sys = (SysDev*)p;
@@ -362,8 +359,6 @@ bool ServerObj::try_launch(Flight& f) {
     if ((size_t)(p - a) > f.arena_bytes) return false;
     for (int i = 0; i < ns; i++) {
         hs[i].scratch = d_spill;
-        hs[i].tailws = d_tailws;
-        hs[i].tailws_stride = (long long)tws;
         hs[i].stats = d_stats + i;
     }
     // Stage the inputs in pinned memory and move them in one copy.

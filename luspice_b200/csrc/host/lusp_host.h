@@ -59,11 +59,17 @@ struct StaticPattern {
     std::vector<int> lrp, lci;
     std::vector<int> urp, uci;
     // slot -> destination: L slots -> index in the L rows, U slots -> index
-    // in the U rows, diagonal slot -> k.
+    // in the U rows, diagonal slot -> k; -1 for entries of the dense
+    // trailing block (not in the row-major copies).
     std::vector<int> slot_dst;
     std::vector<int> fwd_order, bwd_order;   // level-sorted row orders
     std::vector<int> fwd_lev, bwd_lev;
     int nfwd_levels = 0, nbwd_levels = 0;
+    std::vector<int> bwd_pos;                // row -> index in bwd_order
+    // Level descriptors of the sweeps: nlev x {first row idx, end row idx,
+    // first entry, end entry}, then nlev x log2(lanes per row).
+    std::vector<int> fwd_ldesc, bwd_ldesc;
+    int lev_max_ent = 0, lev_max_rows = 0;  // widest level of either sweep
 
     // SELL-C-sigma copy of A in position space (C = 32): slice s covers
     // sorted rows [32 s, 32 s + 32); entry (r, t) of slice s is at
@@ -87,9 +93,9 @@ struct StaticPattern {
 
     // Dense trailing block: rows and columns [k0, n) are refactored and
     // solved as one dense D x D block (D = dtail = n - k0; 0 = none).  The
-    // sweep orders then list the rows < k0 level-sorted (nfwd_levels /
-    // nbwd_levels count these levels only), followed by the tail rows in
-    // ascending order.
+    // sweep orders then list the rows < k0 level-sorted, followed by the
+    // tail rows in ascending order; the forward sweep has one more level,
+    // the tail rows' entries in the columns before k0.
     int k0 = 0, dtail = 0;
 };
 

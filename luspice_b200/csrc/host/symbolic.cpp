@@ -204,15 +204,17 @@ void levels_and_order(int n, const std::vector<int>& visit,
 }  // namespace
 
 // Trailing block size by a cost model in SM cycles of one refactor plus the
-// triangular solves of one GMRES-IR solve.  The sparse engine costs about a
-// cycle per gathered update plus a latency per level of the column schedule
-// (and of the solve sweeps, which have a similar depth); the dense block
-// costs its multiply-subtract pairs (D^3 / 3) plus a latency per 32-column
-// panel (the panel's own dependency chain and the blocked solves).
+// triangular solves of one GMRES-IR solve (about six LU applications),
+// fitted to measurements on B200: the sparse engine costs about a cycle per
+// gathered update plus a latency per level of the column schedule (the
+// solve sweeps have a similar depth and each application pays it twice);
+// the dense block costs its multiply-subtract pairs (D^3 / 3), the solves'
+// reads of the dense factor (D^2 per application) and a latency per column
+// (the panel chain and the blocked solves).
 int choose_dense_tail(const StaticPattern& S) {
     const int n = S.n;
     if (n < 32) return 0;
-    const double c_upd = 1.0, c_lev = 18000.0, c_pair = 0.05, c_panel = 56000.0;
+    const double c_upd = 1.0, c_lev = 28000.0, c_cube = 0.03, c_sq = 20.0, c_lin = 2500.0;
     // Updates that stay in the sparse engine for a tail starting at k0:
     // those whose dependency column j lies before k0.  Column j feeds
     // |L(:,j)| updates into each of the |U(j,:)| later columns.
@@ -228,8 +230,9 @@ int choose_dense_tail(const StaticPattern& S) {
     int best_d = 0;
     for (int D = 32; D <= std::min(n, kMaxDenseTail); D += 32) {
         const int k0 = n - D;
+        const double d = D;
         const double cost = c_upd * ((double)S.gathered - inside[k0]) + c_lev * levmax[k0] +
-                            c_pair * (double)D * D * D / 3.0 + c_panel * ((D + 31) / 32);
+                            c_cube * d * d * d + c_sq * d * d + c_lin * d;
         if (cost < best) {
             best = cost;
             best_d = D;
@@ -341,13 +344,18 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         S.k0 = n - D;
     }
 
-    // Row-major copies of strict L and strict U.
+    // Row-major copies of strict L and strict U.  Entries inside the dense
+    // trailing block (row and column >= k0) live only in the dense copy.
     {
+        const int k0 = S.k0;
+        auto kept = [k0](int i, int k) { return i < k0 || k < k0; };
         S.lrp.assign(n + 1, 0);
         S.urp.assign(n + 1, 0);
         for (int k = 0; k < n; k++) {
-            for (int p = S.cp[k]; p < S.dg[k]; p++) S.urp[S.ri[p] + 1]++;
-            for (int p = S.dg[k] + 1; p < S.cp[k + 1]; p++) S.lrp[S.ri[p] + 1]++;
+            for (int p = S.cp[k]; p < S.dg[k]; p++)
+                if (kept(S.ri[p], k)) S.urp[S.ri[p] + 1]++;
+            for (int p = S.dg[k] + 1; p < S.cp[k + 1]; p++)
+                if (kept(S.ri[p], k)) S.lrp[S.ri[p] + 1]++;
         }
         for (int i = 0; i < n; i++) {
             S.lrp[i + 1] += S.lrp[i];
@@ -362,6 +370,7 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         for (int k = 0; k < n; k++) {
             for (int p = S.cp[k]; p < S.dg[k]; p++) {
                 const int i = S.ri[p];
+                if (!kept(i, k)) continue;
                 const int d = ucur[i]++;
                 S.uci[d] = k;
                 S.slot_dst[p] = d;
@@ -369,6 +378,7 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
             S.slot_dst[S.dg[k]] = k;
             for (int p = S.dg[k] + 1; p < S.cp[k + 1]; p++) {
                 const int i = S.ri[p];
+                if (!kept(i, k)) continue;
                 const int d = lcur[i]++;
                 S.lci[d] = k;
                 S.slot_dst[p] = d;
@@ -376,7 +386,6 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         }
         // Sweep orders over the rows before the dense tail (all rows when
         // there is none); the tail rows follow in ascending order.
-        const int k0 = S.k0;
         // Forward levels: row i depends on the columns of its L row (< i).
         std::vector<int> visit(k0);
         std::iota(visit.begin(), visit.end(), 0);
@@ -396,6 +405,12 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         for (int i = k0; i < n; i++) {
             S.fwd_order.push_back(i);
             S.bwd_order.push_back(i);
+        }
+        // The tail rows' entries in the columns before k0 form one more
+        // forward level (the dense forward solve follows it).
+        if (k0 > 0 && k0 < n) {
+            S.fwd_lev.push_back(n);
+            S.nfwd_levels++;
         }
         // Store the rows contiguously in level order: row fwd_order[idx] of L
         // occupies [lrp[idx], lrp[idx+1]) (U likewise with bwd_order), so a
@@ -420,8 +435,46 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         relayout(S.fwd_order, S.lrp, S.lci, lmap);
         relayout(S.bwd_order, S.urp, S.uci, umap);
         for (int k = 0; k < n; k++) {
-            for (int p = S.cp[k]; p < S.dg[k]; p++) S.slot_dst[p] = umap[S.slot_dst[p]];
-            for (int p = S.dg[k] + 1; p < S.cp[k + 1]; p++) S.slot_dst[p] = lmap[S.slot_dst[p]];
+            for (int p = S.cp[k]; p < S.dg[k]; p++)
+                if (S.slot_dst[p] >= 0) S.slot_dst[p] = umap[S.slot_dst[p]];
+            for (int p = S.dg[k] + 1; p < S.cp[k + 1]; p++)
+                if (S.slot_dst[p] >= 0) S.slot_dst[p] = lmap[S.slot_dst[p]];
+        }
+        // Per-level descriptors of both sweeps: first row, end row, first
+        // entry, end entry, and log2 of the lanes per row (the power of two
+        // at or above the level's mean row length, at most 32).
+        auto level_desc = [](int nlev, const std::vector<int>& lev, const std::vector<int>& rp,
+                             std::vector<int>& out) {
+            out.assign((size_t)nlev * 5, 0);
+            for (int l = 0; l < nlev; l++) {
+                const int r0 = lev[l], r1 = lev[l + 1];
+                const int e0 = rp[r0], e1 = rp[r1];
+                const int nr = std::max(1, r1 - r0);
+                const int mean = (e1 - e0 + nr - 1) / nr;
+                int lg = 0;
+                while ((1 << lg) < mean && lg < 5) lg++;
+                out[(size_t)l * 4 + 0] = r0;
+                out[(size_t)l * 4 + 1] = r1;
+                out[(size_t)l * 4 + 2] = e0;
+                out[(size_t)l * 4 + 3] = e1;
+                out[(size_t)nlev * 4 + l] = lg;
+            }
+        };
+        level_desc(S.nfwd_levels, S.fwd_lev, S.lrp, S.fwd_ldesc);
+        level_desc(S.nbwd_levels, S.bwd_lev, S.urp, S.bwd_ldesc);
+        // Position of each row in the backward order, and the widest level
+        // of either sweep (entries, rows) for the shared-memory stages.
+        S.bwd_pos.assign(n, 0);
+        for (int idx = 0; idx < n; idx++) S.bwd_pos[S.bwd_order[idx]] = idx;
+        S.lev_max_ent = 0;
+        S.lev_max_rows = 0;
+        for (int l = 0; l < S.nfwd_levels; l++) {
+            S.lev_max_ent = std::max(S.lev_max_ent, S.lrp[S.fwd_lev[l + 1]] - S.lrp[S.fwd_lev[l]]);
+            S.lev_max_rows = std::max(S.lev_max_rows, S.fwd_lev[l + 1] - S.fwd_lev[l]);
+        }
+        for (int l = 0; l < S.nbwd_levels; l++) {
+            S.lev_max_ent = std::max(S.lev_max_ent, S.urp[S.bwd_lev[l + 1]] - S.urp[S.bwd_lev[l]]);
+            S.lev_max_rows = std::max(S.lev_max_rows, S.bwd_lev[l + 1] - S.bwd_lev[l]);
         }
     }
 
