@@ -4,12 +4,13 @@ Workload (one step): the 63x64 power-grid MNA matrix plus 18 Vdd pad rows
 (n = 4050), 50 Newton refactorizations on the same pattern with element
 values perturbed log-normally (sigma = 0.1), each followed by a full solve:
 fp32 factors (frozen pivots) + fp64 GMRES-IR (restart 30, rtol 1e-10), all
-50 systems in one persistent launch.  `value` counts only systems whose
+50 systems in one CUDA graph of three persistent kernels (sparse refactor,
+dense trailing block, solve).  `value` counts only systems whose
 solution is within rel-L2 1e-6 of the fp64 oracle (checked after timing).
 
 Also reported: the plain fp64 GPU path on the same inputs (per request and
 batched), p50/p99 single-request latency, the end-to-end figure through the
-public API with host buffers (e2e), the roofline of the batch kernel, and
+public API with host buffers (e2e), the roofline of the solve kernel, and
 the reference's CPU path (cpu_baseline).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -38,7 +39,7 @@ UNIT = "refactor+solves/s"
 NSYS = 50
 WORKLOAD = ("power-grid MNA n=4050 (63x64 mesh + 18 Vdd pads), 50 Newton refactors on one "
             "pattern (log-normal sigma=0.1 element perturbation), fp32 factor + fp64 GMRES-IR "
-            "(restart 30, rtol 1e-10), one persistent launch per step")
+            "(restart 30, rtol 1e-10), one graph of three persistent kernels per step")
 
 
 def peaks():
@@ -101,8 +102,8 @@ class ClockSampler:
 
 
 def algorithmic_bytes(info, stats, vs=4):
-    """Compulsory bytes of one refactor + GMRES-IR solve (per system), from
-    the pattern sizes and the iteration counts the kernel reported:
+    """Compulsory bytes (refactor part, solve part) summed over the systems,
+    from the pattern sizes and the iteration counts the kernel reported:
       refactor  nnz(A)(8+4) + (n+1)4 + nnz(L+U)(vs+4) + 4n
       trisolve  nnz(L+U)(vs+4) + 2(n+1)4 + 3*8n
       SpMV      nnz(A)(s_v+4) + (n+1)4 + 8n + 8n
@@ -114,9 +115,10 @@ def algorithmic_bytes(info, stats, vs=4):
     tri = lu * (vs + 4) + 2 * (n + 1) * 4 + 3 * 8 * n
     spmv_in = nnz * (vs + 4) + (n + 1) * 4 + 16 * n
     spmv64 = nnz * 12 + (n + 1) * 4 + 16 * n
-    total = 0
+    total_ref, total = 0, 0
     for st in stats:
-        b = refactor
+        total_ref += refactor
+        b = 0
         outer = max(st["outer_iters"], 0)
         inner = max(st["inner_iters"], 0)
         b += max(st["nres"], 1) * (spmv64 + 3 * 8 * n)
@@ -132,7 +134,7 @@ def algorithmic_bytes(info, stats, vs=4):
                 b += spmv_in + tri + 2 * (j + 1) * 2 * 8 * n
             b += outer * tri
         total += b
-    return total
+    return total_ref, total
 
 
 def ref_cpu_worker(args):
@@ -282,12 +284,27 @@ def main():
         accepted += int(e <= 1e-6)
     value = accepted * world / (step_ms / 1000.0)
 
-    # Roofline of the batch kernel (the only kernel of the step).
+    # Roofline of the dominant kernel, the solve kernel (level-scheduled
+    # triangular solves, dense-tail solves, SpMV, GMRES-IR): timed alone
+    # with events on its stream, L2 flushed before each launch, after a
+    # refactor of the same values.
     hbm, peak_kind = peaks()
-    alg = algorithmic_bytes(info, stats, vs=4)
-    achieved = alg / (statistics.mean(kern_ms) / 1000.0) / 1e9
+    alg_ref, alg = algorithmic_bytes(info, stats, vs=4)
+    sol_ms = []
+    for i in range(max(3, args.steps // 2)):
+        B.run(api.RUN_REFACTOR, stream=stream)
+        a, bq = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.fill_(float(i))
+            a.record(stream)
+        B.run(api.RUN_SOLVE, stream=stream)
+        bq.record(stream)
+        torch.cuda.synchronize()
+        sol_ms.append(a.elapsed_time(bq))
+    solve_ms = statistics.mean(sol_ms)
+    achieved = alg / (solve_ms / 1000.0) / 1e9
     traffic = None
-    prof = ROOT / "profiles" / "batch_kernel_power_grid4050x50.json"
+    prof = ROOT / "profiles" / "solve_kernel_power_grid4050x50.json"
     if prof.exists():
         traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
 
@@ -376,7 +393,8 @@ def main():
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "batch_kernel<float,float>", "alg_bytes_per_launch": alg},
+                         "kernel": "solve_kernel<float,float>", "alg_bytes_per_launch": alg,
+                         "kernel_ms": solve_ms, "refactor_alg_bytes_per_step": alg_ref},
             "gpu_launches": args.steps * B.launch_count(),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
