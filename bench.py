@@ -183,13 +183,8 @@ def setup_dist(n_gpus):
 
 
 def max_over_ranks(v, world):
-    if world <= 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from luspice_b200.shard import max_over_ranks as mor
+    return mor(v, world)
 
 
 def barrier(world):
