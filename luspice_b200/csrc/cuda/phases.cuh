@@ -677,20 +677,21 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
 // (column-major factor): all loads issued before the multiply-adds.
 template <typename VT>
 __device__ __forceinline__ double tail_row_dot(const VT* row, size_t stride, const double* y, int w) {
+    // Unconditional loads from clamped (in-bounds) addresses, so all 32 are
+    // in flight before the first multiply-add.
     VT v[32];
 #pragma unroll
-    for (int c = 0; c < 32; c++) v[c] = c < w ? row[c * stride] : VT(0);
+    for (int c = 0; c < 32; c++) v[c] = row[(size_t)min(c, w - 1) * stride];
     double acc = 0.0;
 #pragma unroll
-    for (int c = 0; c < 32; c++)
-        if (c < w) acc = fma((double)v[c], y[c], acc);
+    for (int c = 0; c < 32; c++) acc = fma(c < w ? (double)v[c] : 0.0, y[min(c, w - 1)], acc);
     return acc;
 }
 
 // y[k0..n) := L_tt^-1 y[k0..n) (unit lower; the tail rows' entries in the
 // columns before k0 were applied by the forward sweep's last level).
 template <typename VT>
-__device__ void tail_forward(const PatternDev& P, const VT* T, double* y, SysStats* st) {
+__device__ __noinline__ void tail_forward(const PatternDev& P, const VT* T, double* y, SysStats* st) {
     const int k0 = P.k0, D = P.dtail, ld = P.tail_ld;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     long long c_diag = 0, c_gemv = 0;
@@ -700,10 +701,13 @@ __device__ void tail_forward(const PatternDev& P, const VT* T, double* y, SysSta
         const long long ta = clock64();
         if (warp == 0) {
             double lr[32];
-            const VT* row = T + (size_t)jb * ld + jb + lane;
+            const int lr_ = min(lane, w - 1);
+            const VT* row = T + (size_t)jb * ld + jb + lr_;
 #pragma unroll
-            for (int c = 0; c < 32; c++)
-                lr[c] = (c < lane && lane < w) ? ValTraits<VT>::load(row + (size_t)c * ld) : 0.0;
+            for (int c = 0; c < 32; c++) {
+                const double v = ValTraits<VT>::load(row + (size_t)min(c, w - 1) * ld);
+                lr[c] = (c < lane && lane < w) ? v : 0.0;
+            }
             double yr = lane < w ? yt[jb + lane] : 0.0;
 #pragma unroll
             for (int c = 0; c < 31; c++) {
@@ -729,7 +733,7 @@ __device__ void tail_forward(const PatternDev& P, const VT* T, double* y, SysSta
 
 // y[k0..n) := U_tt^-1 y[k0..n) (upper with diagonal).
 template <typename VT>
-__device__ void tail_backward(const PatternDev& P, const VT* T, double* y, SysStats* st) {
+__device__ __noinline__ void tail_backward(const PatternDev& P, const VT* T, double* y, SysStats* st) {
     const int k0 = P.k0, D = P.dtail, ld = P.tail_ld;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     long long c_diag = 0, c_gemv = 0;
@@ -739,11 +743,15 @@ __device__ void tail_backward(const PatternDev& P, const VT* T, double* y, SysSt
         const long long ta = clock64();
         if (warp == 0) {
             double ur[32];
-            const VT* row = T + (size_t)jb * ld + jb + lane;
+            const int lr_ = min(lane, w - 1);
+            const VT* row = T + (size_t)jb * ld + jb + lr_;
 #pragma unroll
-            for (int c = 0; c < 32; c++)
-                ur[c] = (c > lane && c < w) ? ValTraits<VT>::load(row + (size_t)c * ld) : 0.0;
-            const double dg = lane < w ? ValTraits<VT>::load(row + (size_t)lane * ld) : 1.0;
+            for (int c = 0; c < 32; c++) {
+                const double v = ValTraits<VT>::load(row + (size_t)min(c, w - 1) * ld);
+                ur[c] = (c > lane && c < w) ? v : 0.0;
+            }
+            const double dgv = ValTraits<VT>::load(row + (size_t)lr_ * ld);
+            const double dg = lane < w ? dgv : 1.0;
             double yr = lane < w ? yt[jb + lane] : 0.0;
 #pragma unroll
             for (int c = 31; c >= 0; c--) {
