@@ -182,7 +182,7 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
                                         &S.lrp, &S.lci, &S.urp, &S.uci, &S.slot_dst, &S.fwd_order,
                                         &S.bwd_order, &S.sell_ptr, &S.sell_col, &S.sell_src,
                                         &S.sell_perm, &S.rowat, &S.q, &S.fwd_lev, &S.bwd_lev, &S.bwd_pos,
-                                        &S.fwd_ldesc, &S.bwd_ldesc};
+                                        &S.fwd_ldesc, &S.bwd_ldesc, &S.dep_bc};
     const int narr = (int)(sizeof(arrays) / sizeof(arrays[0]));
     std::vector<size_t> off(narr + 1, 0);
     // Each array gets at least 8 ints of slack: the sweeps copy index runs
@@ -232,6 +232,7 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     D.bwd_pos = blk + off[idx++];
     D.fwd_ldesc = blk + off[idx++];
     D.bwd_ldesc = blk + off[idx++];
+    D.dep_bc = (const int2*)(blk + off[idx++]);
     D.lev_max_ent = S.lev_max_ent;
     D.lev_max_rows = S.lev_max_rows;
     D.nfwd_levels = S.nfwd_levels;

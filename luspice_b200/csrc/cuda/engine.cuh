@@ -41,6 +41,8 @@ struct PatternDev {
     const int* sell_perm;    // [32*nslices] row position or -1
     const int* rowat;        // [n] position -> original row
     const int* q;            // [n] position -> original column
+    const int2* dep_bc;           // [cap] for U slots: {first strict-L slot,
+                                  // strict-L length} of the dependency column
     const unsigned short* rel;    // relative update slots (null: search rows)
     const long long* rel_ptr;     // [n+1] column k's list in rel
     // Dense trailing block: rows/columns [k0, n), dtail = n - k0 (0: none),

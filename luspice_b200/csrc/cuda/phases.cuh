@@ -511,15 +511,19 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
             bool rdy = true;
             if (u < dsp) {
                 const int jj = rows[u];
-                beg = P.dg[jj] + 1;
-                cnt = P.cp[jj + 1] - beg;
+                const int2 bc = P.dep_bc[c0 + u];
+                beg = bc.x;
+                cnt = bc.y;
                 rdy = is_ready(sm.ready, jj);
             }
             int nready = __ffs(~__ballot_sync(0xffffffffu, rdy)) - 1;
             if (nready < 0) nready = 32;
             if (nready == 0) {
-                if (!wait_ready(sm.ready, rows[u0], &sm.ctl[3])) bad |= ST_WAIT_TIMEOUT;
-                __syncwarp();
+                // Wait for the next dependency, then re-scan: others may
+                // have completed meanwhile and join the same round.
+                const bool ok = __all_sync(0xffffffffu, wait_ready(sm.ready, rows[u0], &sm.ctl[3]));
+                if (ok) continue;
+                bad |= ST_WAIT_TIMEOUT;
                 nready = 1;
             }
             __threadfence_block();

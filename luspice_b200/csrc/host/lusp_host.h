@@ -90,6 +90,9 @@ struct StaticPattern {
     // Empty when a column is longer than 65535 slots.
     std::vector<uint16_t> rel;
     std::vector<long long> rel_ptr;
+    // For each U slot p of column k (row j): {dg[j] + 1, cp[j+1] - dg[j] - 1},
+    // the strict-L part of the dependency column (2 ints per slot, all slots).
+    std::vector<int> dep_bc;
 
     // Dense trailing block: rows and columns [k0, n) are refactored and
     // solved as one dense D x D block (D = dtail = n - k0; 0 = none).  The

@@ -307,6 +307,15 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         S.gathered = ga;
     }
 
+    // Dependency metadata per U slot.
+    S.dep_bc.assign((size_t)S.cap * 2, 0);
+    for (int k = 0; k < n; k++)
+        for (int p = S.cp[k]; p < S.dg[k]; p++) {
+            const int j = S.ri[p];
+            S.dep_bc[(size_t)p * 2] = S.dg[j] + 1;
+            S.dep_bc[(size_t)p * 2 + 1] = S.cp[j + 1] - S.dg[j] - 1;
+        }
+
     // Relative update slots (16 bit), built through a row -> slot table of
     // the current column.
     S.rel.clear();
