@@ -515,7 +515,7 @@ size_t system_private_bytes(const StaticPattern& S, size_t vs, int m) {
     // The row-major values and the sweep-order diagonal get 64 bytes of
     // slack: the sweeps copy them in aligned 16-byte pieces.
     return al256(S.cap * vs) + al256(S.lci.size() * vs + 64) + al256(S.uci.size() * vs + 64) + al256(n * vs) +
-           al256(n * vs + 64) + al256(st * 8) + al256(st * 4) + al256(((size_t)m + 8) * n * 8) +
+           al256(n * vs + 64) + al256(st * 8) + al256(st * 4) + al256((2 * (size_t)m + 8) * n * 8) +
            al256((size_t)S.dtail * tail_ld(S) * vs) + al256((size_t)S.dtail * tail_ld(S) * 8);
 }
 
@@ -532,7 +532,7 @@ char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m)
     D.udiag_bwd = p; p += al256(n * vs + 64);
     D.sell64 = (double*)p; p += al256(st * 8);
     D.sell32 = (float*)p; p += al256(st * 4);
-    D.work = (double*)p; p += al256(((size_t)m + 8) * n * 8);
+    D.work = (double*)p; p += al256((2 * (size_t)m + 8) * n * 8);
     return p;
 }
 

@@ -1168,6 +1168,7 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
     double* yg = w + n;
     double* V = yg + n;
     double* xprev = V + (size_t)(m + 1) * n;   // iterate before the last correction
+    double* Zb = xprev + n;                      // [m x n] preconditioned basis z_j = M^-1 v_j
     // Shared: y (optional) | H[(m+1) x m] | g, cs, sn, h, h2, yc
     double* ys = (double*)sm.uni;
     double* H = ys + plan.ycap;
@@ -1255,6 +1256,10 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         for (int j = 0; j < m; j++) {
             const double* vj = V + (size_t)j * n;
             lu_apply<VT>(S, plan, vj, y, sm, desc, bad);
+            // Keep z_j: the correction is then sum_i y_i z_i, without
+            // another preconditioner application (flexible-GMRES layout).
+            double* zj = Zb + (size_t)j * n;
+            for (int e = threadIdx.x; e < n; e += blockDim.x) zj[e] = y[e];
             const long long tsp = clock64();
             cta_spmv<AT, false>(P, ainner, y, nullptr, w);
             __syncthreads();
@@ -1321,11 +1326,10 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         __syncthreads();
         for (int e = threadIdx.x; e < n; e += blockDim.x) {
             double acc = 0.0;
-            for (int i = 0; i < jj; i++) acc = fma(yc[i], V[(size_t)i * n + e], acc);
-            z[e] = acc;
+            for (int i = 0; i < jj; i++) acc = fma(yc[i], Zb[(size_t)i * n + e], acc);
+            y[e] = acc;
         }
         __syncthreads();
-        lu_apply<VT>(S, plan, z, y, sm, desc, bad);
         double sy = 0.0, sx = 0.0;
         for (int e = threadIdx.x; e < n; e += blockDim.x) {
             xprev[e] = xt[e];
