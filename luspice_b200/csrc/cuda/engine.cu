@@ -512,9 +512,9 @@ int tail_ld(const StaticPattern& S) { return (S.dtail + 31) & ~31; }
 size_t system_private_bytes(const StaticPattern& S, size_t vs, int m) {
     const size_t n = S.n;
     const size_t st = S.sell_ptr.back();
-    // The row-major values and the sweep-order diagonal get 64 bytes of
-    // slack: the sweeps copy them in aligned 16-byte pieces.
-    return al256(S.cap * vs) + al256(S.lci.size() * vs + 64) + al256(S.uci.size() * vs + 64) + al256(n * vs) +
+    // The merged and row-major values and the sweep-order diagonal get 64
+    // bytes of slack: the kernels copy them in aligned 16-byte pieces.
+    return al256(S.cap * vs + 64) + al256(S.lci.size() * vs + 64) + al256(S.uci.size() * vs + 64) + al256(n * vs) +
            al256(n * vs + 64) + al256(st * 8) + al256(st * 4) + al256((2 * (size_t)m + 8) * n * 8) +
            al256((size_t)S.dtail * tail_ld(S) * vs) + al256((size_t)S.dtail * tail_ld(S) * 8);
 }
@@ -525,7 +525,7 @@ char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m)
     D.tail = p; p += al256((size_t)S.dtail * tail_ld(S) * vs);
     D.tailw = S.dtail > 0 ? (double*)p : nullptr;
     p += al256((size_t)S.dtail * tail_ld(S) * 8);
-    D.lu = p; p += al256(S.cap * vs);
+    D.lu = p; p += al256(S.cap * vs + 64);
     D.lval = p; p += al256(S.lci.size() * vs + 64);
     D.uval = p; p += al256(S.uci.size() * vs + 64);
     D.udiag = p; p += al256(n * vs);

@@ -539,7 +539,23 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 if (lane >= o) incl += v;
             }
             const int excl = incl - cnt;
-            int nfit = have_rel ? __popc(__ballot_sync(0xffffffffu, u < dsp && incl <= plan.scap)) : 0;
+            // Value stage layout: each dependency's run starts at the 16-byte
+            // boundary at or below its first value (copied in whole 16-byte
+            // pieces that bypass L1, so values written by another SM are never
+            // read from a stale L1 line).
+            constexpr int VPK = 16 / (int)sizeof(VT);
+            const int vsh = beg & (VPK - 1);
+            const int vlen = u < dsp ? ((vsh + cnt + VPK - 1) / VPK) * VPK : 0;
+            int vincl = vlen;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, vincl, o);
+                if (lane >= o) vincl += v;
+            }
+            const int vexcl = vincl - vlen;
+            int nfit = have_rel ? __popc(__ballot_sync(0xffffffffu, u < dsp && incl <= plan.scap &&
+                                                                        vincl <= plan.scap))
+                                : 0;
             nfit = min(nfit, nready);
             if (nfit == 0) {
                 // One dependency applied straight from global memory (longer
@@ -549,7 +565,7 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 const int c = __shfl_sync(0xffffffffu, cnt, 0);
                 if (xj != 0.0) {
                     for (int e = lane; e < c; e += 32) {
-                        const double l = ValTraits<VT>::load(lu + p0 + e);
+                        const double l = (double)__ldcg(lu + p0 + e);
                         const int s = have_rel ? (int)P.rel[roff + e]
                                                : find_slot(rows, u0 + 1, len, P.ri[p0 + e]);
                         if (s >= 0) x[s] = __dsub_rn(x[s], __dmul_rn(l, xj));
@@ -569,10 +585,10 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
             const int pieces = (sh + tot + 7) >> 3;
             for (int e = lane; e < pieces; e += 32) cp_async_16(srel + 8 * e, P.rel + g0 + 8 * e);
             for (int t = 0; t < nfit; t++) {
-                const int b_t = __shfl_sync(0xffffffffu, beg, t);
-                const int c_t = __shfl_sync(0xffffffffu, cnt, t);
-                const int o_t = __shfl_sync(0xffffffffu, excl, t);
-                for (int e = lane; e < c_t; e += 32) cp_async_val(sval + o_t + e, lu + b_t + e);
+                const int a_t = __shfl_sync(0xffffffffu, beg - vsh, t);
+                const int p_t = __shfl_sync(0xffffffffu, vlen, t) / VPK;
+                const int o_t = __shfl_sync(0xffffffffu, vexcl, t);
+                for (int e = lane; e < p_t; e += 32) cp_async_16(sval + o_t + e * VPK, lu + a_t + e * VPK);
             }
             cp_async_wait_all();
             __syncwarp();
@@ -584,6 +600,7 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
             for (int t = 0; t < nfit; t++) {
                 const int c_t = __shfl_sync(0xffffffffu, cnt, t);
                 const int o_t = __shfl_sync(0xffffffffu, excl, t);
+                const int vo_t = __shfl_sync(0xffffffffu, vexcl + vsh, t);
                 const double xj = x[u0 + t];
                 if (xj != 0.0) {
                     // Rows of one dependency are distinct: four entries per
@@ -595,7 +612,7 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                         for (int q = 0; q < 4; q++) {
                             const int ee = e + 32 * q;
                             s[q] = ee < c_t ? (int)srel[sh + o_t + ee] : -1;
-                            l[q] = ee < c_t ? ValTraits<VT>::load(sval + o_t + ee) : 0.0;
+                            l[q] = ee < c_t ? ValTraits<VT>::load(sval + vo_t + ee) : 0.0;
                         }
 #pragma unroll
                         for (int q = 0; q < 4; q++) xv[q] = s[q] >= 0 ? x[s[q]] : 0.0;
