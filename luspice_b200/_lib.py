@@ -41,7 +41,8 @@ class BatchOpts(C.Structure):
                 ("rtol", C.c_double), ("inner_rel", C.c_double), ("stag_ratio", C.c_double),
                 ("pivot_tol", C.c_double), ("block_threads", C.c_int), ("ctas_per_sm", C.c_int),
                 ("solve_sweep", C.c_int), ("refactor_mode", C.c_int), ("inner_prec", C.c_int),
-                ("xtol", C.c_double), ("refactor_threads", C.c_int)]
+                ("xtol", C.c_double), ("refactor_threads", C.c_int),
+                ("refactor_cluster", C.c_int)]
 
 
 class ServerOpts(C.Structure):

@@ -161,6 +161,7 @@ void lusp_batch_opts_default(lusp_batch_opts* o) {
     o->inner_prec = 0;
     o->xtol = 1e-8;
     o->refactor_threads = 0;
+    o->refactor_cluster = 0;
 }
 
 int lusp_batch_create(int nsys, lusp_pattern* const* pats, const lusp_batch_opts* opts,

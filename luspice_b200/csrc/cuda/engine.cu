@@ -56,11 +56,18 @@ __global__ void __launch_bounds__(1024, 1)
 refactor_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan, SolveParams prm) {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_task;
+    // A thread-block cluster (or a lone CTA) takes one system at a time:
+    // rank 0 draws it, every CTA reads it through distributed shared memory
+    // between two cluster barriers (so rank 0 outlives the read).
+    namespace cgr = cooperative_groups;
+    cgr::cluster_group cl = cgr::this_cluster();
+    const volatile int* task0 = cl.map_shared_rank(&s_task, 0);
     while (true) {
-        __syncthreads();
-        if (threadIdx.x == 0) s_task = atomicAdd(queue, 1);
-        __syncthreads();
-        const int t = s_task;
+        cl.sync();
+        if (cl.block_rank() == 0 && threadIdx.x == 0) s_task = atomicAdd(queue, 1);
+        cl.sync();
+        const int t = *task0;
+        cl.sync();
         if (t >= nsys) break;
         const SysDev S = sys[t];
         refactor_phase<VT>(S, plan, smem, prm);
@@ -439,6 +446,27 @@ static int refactor_prepare(size_t smem, int block, int* occ) {
     return prepare_kernel(refactor_kernel<VT>, smem, block, occ, &granted, mu);
 }
 
+// Clusters of csize refactor CTAs that can be resident at once.
+template <typename VT>
+static int refactor_cluster_count(size_t smem, int block, int csize, int* nclusters) {
+    int rc = refactor_prepare<VT>(smem, block, nullptr);
+    if (rc != LUSP_OK) return rc;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)csize * sm_count());
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(nclusters, refactor_kernel<VT>, &cfg);
+    if (e != cudaSuccess) return cuda_fail(e, "cluster occupancy query");
+    return LUSP_OK;
+}
+
 template <typename VT>
 static int dense_prepare(size_t smem, int block, int* occ) {
     static std::mutex mu;
@@ -464,8 +492,25 @@ static int launch_typed(const LaunchArgs& a, cudaStream_t st) {
     if (a.what & LUSP_RUN_REFACTOR) {
         int rc = refactor_prepare<VT>(a.rplan.bytes, a.rblock, nullptr);
         if (rc != LUSP_OK) return rc;
-        refactor_kernel<VT><<<a.rgrid, a.rblock, a.rplan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.rplan, a.prm);
-        e = cudaGetLastError();
+        if (a.rcluster > 1) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)a.rgrid);
+            cfg.blockDim = dim3((unsigned)a.rblock);
+            cfg.dynamicSmemBytes = a.rplan.bytes;
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = (unsigned)a.rcluster;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            e = cudaLaunchKernelEx(&cfg, refactor_kernel<VT>, a.d_sys, a.nsys, a.d_queue, a.rplan, a.prm);
+        } else {
+            refactor_kernel<VT><<<a.rgrid, a.rblock, a.rplan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.rplan,
+                                                                          a.prm);
+            e = cudaGetLastError();
+        }
         if (e != cudaSuccess) return cuda_fail(e, "refactor kernel launch");
         if (a.dgrid > 0) {
             rc = dense_prepare<VT>(a.dplan.bytes, a.dblock, nullptr);
@@ -549,6 +594,10 @@ int check_opts(const lusp_batch_opts* o) {
     }
     if (o->ctas_per_sm < 0) { set_error("ctas_per_sm must be >= 0"); return LUSP_EARG; }
     if (o->inner_prec < 0 || o->inner_prec > 1) { set_error("bad inner_prec"); return LUSP_EARG; }
+    if (o->refactor_cluster < 0 || o->refactor_cluster > 8) {
+        set_error("refactor_cluster must be 0 (auto) or 1..8");
+        return LUSP_EARG;
+    }
     if (o->refactor_threads != 0 &&
         (o->refactor_threads < 64 || o->refactor_threads > 1024 || o->refactor_threads % 32)) {
         set_error("refactor_threads must be 0 (auto) or 64..1024, a multiple of 32");
@@ -576,6 +625,22 @@ int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& 
     if (rc != LUSP_OK) return rc;
     if (occ < 1) { set_error("refactor kernel does not fit one SM (smem %zu)", a.rplan.bytes); return LUSP_EARG; }
     a.rgrid = std::min(nsys, occ * sm_count());
+    // Spread a system's columns over a cluster of CTAs when every system of
+    // the batch still gets its own cluster at once (the refactor is bound by
+    // instruction issue on one SM; the dependency chain leaves room).
+    a.rcluster = 1;
+    int want = o.refactor_cluster;
+    if (want == 0) want = (a.rblock == 1024 && 2 * nsys <= sm_count()) ? 2 : 1;
+    if (want > 1) {
+        int ncl = 0;
+        rc = o.prec == LUSP_FP64 ? refactor_cluster_count<double>(a.rplan.bytes, a.rblock, want, &ncl)
+                                 : refactor_cluster_count<float>(a.rplan.bytes, a.rblock, want, &ncl);
+        if (rc != LUSP_OK) return rc;
+        if (ncl >= 1 && (o.refactor_cluster > 1 || ncl >= nsys)) {
+            a.rcluster = want;
+            a.rgrid = want * std::min(nsys, ncl);
+        }
+    }
     // Dense trailing blocks: their own kernel when any system has one.
     int ntail = 0;
     for (auto* p : pats) ntail += p->S.dtail > 0 ? 1 : 0;

@@ -38,6 +38,7 @@ struct LaunchArgs {
     SmemPlan rplan{};                // refactorization kernel
     int rblock = 1024;
     int rgrid = 1;
+    int rcluster = 1;                // CTAs per system (thread-block cluster)
     SmemPlan dplan{};                // dense trailing-block kernel (dgrid 0: none)
     int dblock = 512;
     int dgrid = 0;

@@ -2,6 +2,8 @@
 // level-scheduled triangular solves, SELL SpMV, Arnoldi and the GMRES-IR
 // driver.  Every function here is called by all threads of the CTA.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "engine.cuh"
 
 namespace lusp {
@@ -55,6 +57,15 @@ __device__ __forceinline__ void cp_async_val(float* sdst, const float* gsrc) { c
 __device__ __forceinline__ void cp_async_val(double* sdst, const double* gsrc) { cp_async_8(sdst, gsrc); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Orders this thread's memory operations for the other CTAs sharing a
+// system: block scope for a lone CTA, cluster scope when the system's
+// columns are spread over a thread-block cluster (release before publishing
+// a ready bit, acquire after observing one).
+__device__ __forceinline__ void share_fence(unsigned csize) {
+    if (csize > 1) asm volatile("fence.acq_rel.cluster;\n" ::: "memory");
+    else __threadfence_block();
+}
+
 __device__ __forceinline__ int warp_claim(int* counter) {
     int idx = 0;
     if ((threadIdx.x & 31) == 0) idx = atomicAdd(counter, 1);
@@ -64,9 +75,10 @@ __device__ __forceinline__ int warp_claim(int* counter) {
 // Pivot statistics of a CTA: warp reductions, then per-warp partials
 // combined in order by thread 0.  first: overwrite the system's statistics
 // (refactor kernel), else merge into them (dense trailing-block kernel).
-// Status bits go through sm.ctl[1], the singular column through sm.ctl[2].
+// Status bits go through ctl[1], the singular column through ctl[2] (the
+// CTA's own control words, or those of the cluster's rank 0).
 __device__ void cta_store_pivot_stats(SysStats* st, Smem& sm, double minpiv, double minratio, double maxu,
-                                      int bad, bool first) {
+                                      int bad, bool first, int* ctl) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     minpiv = warp_min(minpiv);
     minratio = warp_min(minratio);
@@ -75,7 +87,7 @@ __device__ void cta_store_pivot_stats(SysStats* st, Smem& sm, double minpiv, dou
     __syncthreads();
     if (lane == 0) {
         sm.red[warp] = minpiv;
-        atomicOr(&sm.ctl[1], bad);
+        atomicOr(&ctl[1], bad);
     }
     __syncthreads();
     double a = INFINITY;
@@ -93,12 +105,13 @@ __device__ void cta_store_pivot_stats(SysStats* st, Smem& sm, double minpiv, dou
     if (threadIdx.x == 0) {
         double c = 0.0;
         for (int w = 0; w < nw; w++) c = fmax(c, sm.red[w]);
-        const int sc = sm.ctl[2] == 0x7fffffff ? -1 : sm.ctl[2];
+        const int c2 = *(volatile int*)&ctl[2];
+        const int sc = c2 == 0x7fffffff ? -1 : c2;
         if (first) {
             st->min_abs_pivot = a;
             st->min_pivot_ratio = b;
             st->max_abs_u = c;
-            st->status = sm.ctl[1];
+            st->status = *(volatile int*)&ctl[1];
             st->singular_col = sc;
             st->nres = 0;
             st->inner_iters = 0;
@@ -107,7 +120,7 @@ __device__ void cta_store_pivot_stats(SysStats* st, Smem& sm, double minpiv, dou
             st->min_abs_pivot = fmin(st->min_abs_pivot, a);
             st->min_pivot_ratio = fmin(st->min_pivot_ratio, b);
             st->max_abs_u = fmax(st->max_abs_u, c);
-            st->status |= sm.ctl[1];
+            st->status |= *(volatile int*)&ctl[1];
             if (sc >= 0 && (st->singular_col < 0 || sc < st->singular_col)) st->singular_col = sc;
         }
     }
@@ -381,7 +394,7 @@ __device__ void dense_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
     dense_tail_factor<VT>(P, S.tailw, sm, plan, prm, minpiv, minratio, bad, S.stats);
     __syncthreads();
     dense_tail_store<VT>(S, P, S.tailw, maxu, sm.uni, plan.ttw);
-    cta_store_pivot_stats(S.stats, sm, minpiv, minratio, maxu, bad, false);
+    cta_store_pivot_stats(S.stats, sm, minpiv, minratio, maxu, bad, false, sm.ctl);
 }
 
 // ---------------------------------------------------------------------------
@@ -419,27 +432,37 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
     VT* sval = (VT*)(wbase + (size_t)plan.wcap * 8);
     unsigned short* srel = (unsigned short*)(wbase + (size_t)plan.wcap * 8 + (size_t)plan.scap * sizeof(VT));
     const bool have_rel = P.rel != nullptr && prm.refactor_mode == 0;
+    // The CTAs of a thread-block cluster share one system: the claim
+    // counter, status, singular column, abort flag and ready bits live in
+    // rank 0's shared memory (distributed shared memory for the others).
+    namespace cgr = cooperative_groups;
+    cgr::cluster_group cl = cgr::this_cluster();
+    const unsigned crank = cl.block_rank(), csize = cl.num_blocks();
+    unsigned* ready = cl.map_shared_rank(sm.ready, 0);
+    int* ctl = cl.map_shared_rank(sm.ctl, 0);
 
-    for (int t = threadIdx.x; t < (n + 31) / 32; t += blockDim.x) sm.ready[t] = 0u;
-    if (threadIdx.x == 0) {
-        sm.ctl[0] = 0;
-        sm.ctl[1] = 0;
-        sm.ctl[2] = 0x7fffffff;
-        sm.ctl[3] = 0;
+    if (crank == 0) {
+        for (int t = threadIdx.x; t < (n + 31) / 32; t += blockDim.x) sm.ready[t] = 0u;
+        if (threadIdx.x == 0) {
+            sm.ctl[0] = 0;
+            sm.ctl[1] = 0;
+            sm.ctl[2] = 0x7fffffff;
+            sm.ctl[3] = 0;
+        }
     }
+    const int gt = (int)(crank * blockDim.x + threadIdx.x), gs = (int)(csize * blockDim.x);
     // A in SELL order for the solves: fp64 (outer residual) and fp32 (inner).
-    for (int t = threadIdx.x; t < P.sell_total; t += blockDim.x) {
+    for (int t = gt; t < P.sell_total; t += gs) {
         const int s = P.sell_src[t];
         const double v = s >= 0 ? S.a_val[s] : 0.0;
         S.sell64[t] = v;
         S.sell32[t] = (float)v;
     }
-    // This CTA's dense trailing block, zeroed: the tail columns scatter only
-    // their pattern's entries into it.
+    // The system's dense trailing block, zeroed: the tail columns scatter
+    // only their pattern's entries into it.
     double* W = P.dtail > 0 ? S.tailw : nullptr;
     if (W)
-        for (size_t t = threadIdx.x; t < (size_t)P.dtail * P.tail_ld; t += blockDim.x) W[t] = 0.0;
-    __syncthreads();
+        for (size_t t = gt; t < (size_t)P.dtail * P.tail_ld; t += gs) W[t] = 0.0;
 
     VT* lu = (VT*)S.lu;
     VT* lval = (VT*)S.lval;
@@ -449,15 +472,15 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
     int bad = 0;
     long long c_wait = 0, c_gather = 0, c_update = 0;
     const long long t_begin = clock64();
-    if (threadIdx.x == 0) {
+    if (crank == 0 && threadIdx.x == 0) {
         S.stats->cyc_wait = 0;
         S.stats->cyc_gather = 0;
         S.stats->cyc_update = 0;
     }
-    __syncthreads();
+    cl.sync();
 
     while (true) {
-        const int idx = warp_claim(&sm.ctl[0]);
+        const int idx = warp_claim(&ctl[0]);
         if (idx >= n) break;
         const int k = P.col_order[idx];
         const int c0 = P.cp[k], c1 = P.cp[k + 1];
@@ -471,7 +494,7 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         } else {
             bad |= ST_CAPACITY;
             __syncwarp();
-            if (lane == 0) set_ready(sm.ready, k);
+            if (lane == 0) set_ready(ready, k);
             continue;
         }
         // A column of the dense trailing block applies only its dependencies
@@ -514,19 +537,21 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 const int2 bc = P.dep_bc[c0 + u];
                 beg = bc.x;
                 cnt = bc.y;
-                rdy = is_ready(sm.ready, jj);
+                rdy = is_ready(ready, jj);
             }
             int nready = __ffs(~__ballot_sync(0xffffffffu, rdy)) - 1;
             if (nready < 0) nready = 32;
             if (nready == 0) {
                 // Wait for the next dependency, then re-scan: others may
                 // have completed meanwhile and join the same round.
-                const bool ok = __all_sync(0xffffffffu, wait_ready(sm.ready, rows[u0], &sm.ctl[3]));
+                const bool ok = __all_sync(0xffffffffu, wait_ready(ready, rows[u0], &ctl[3]));
                 if (ok) continue;
                 bad |= ST_WAIT_TIMEOUT;
                 nready = 1;
             }
-            __threadfence_block();
+            // Acquire: the dependency columns' values (written by any CTA of
+            // the cluster) are read after their ready bits.
+            share_fence(csize);
             {
                 const long long t2 = clock64();
                 c_wait += t2 - tc;
@@ -654,7 +679,7 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         const double ap = fabs(piv);
         if (!(ap > 0.0) || !isfinite(piv)) {
             bad |= ST_SINGULAR;
-            if (lane == 0) atomicMin(&sm.ctl[2], k);
+            if (lane == 0) atomicMin(&ctl[2], k);
         }
         minpiv = fmin(minpiv, ap);
         const double ratio = amax > ap ? ap / amax : 1.0;
@@ -674,9 +699,10 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 ((VT*)S.udiag_bwd)[P.bwd_pos[k]] = ValTraits<VT>::to(1.0 / piv);
             } else lval[dst] = sv;
         }
-        __threadfence_block();
+        // Release: the column's values before its ready bit.
+        share_fence(csize);
         __syncwarp();
-        if (lane == 0) set_ready(sm.ready, k);
+        if (lane == 0) set_ready(ready, k);
     }
 
     if (lane == 0) {
@@ -685,7 +711,14 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         atomicAdd((unsigned long long*)&S.stats->cyc_update, (unsigned long long)c_update);
     }
     if (threadIdx.x == 0) S.stats->cyc_refactor = clock64() - t_begin;
-    cta_store_pivot_stats(S.stats, sm, minpiv, minratio, maxu, bad, true);
+    // Statistics: rank 0 writes, the others merge, one after another; the
+    // last cluster barrier also keeps rank 0's shared state alive until every
+    // CTA of the cluster is done with it.
+    cl.sync();
+    for (unsigned r = 0; r < csize; r++) {
+        if (crank == r) cta_store_pivot_stats(S.stats, sm, minpiv, minratio, maxu, bad, r == 0, ctl);
+        cl.sync();
+    }
 }
 
 // ---------------------------------------------------------------------------
