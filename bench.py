@@ -37,6 +37,9 @@ sys.path.insert(0, str(ROOT))
 METRIC = "refactor+solves/s at rel err ≤1e-6 (mixed vs fp64 GPU); p50/p99 solve latency"
 UNIT = "refactor+solves/s"
 NSYS = 50
+# Device-side spin (SM cycles, ~0.1 ms) enqueued before a timed interval so
+# the host has queued the timed work before the GPU reaches it.
+HOST_AHEAD_CYCLES = 200_000
 WORKLOAD = ("power-grid MNA n=4050 (63x64 mesh + 18 Vdd pads), 50 Newton refactors on one "
             "pattern (log-normal sigma=0.1 element perturbation), fp32 factor + fp64 GMRES-IR "
             "(restart 30, rtol 1e-10), one graph of three persistent kernels per step")
@@ -214,6 +217,225 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# --suite: the other workloads of the path, one JSON line each (not part of
+# the default run): uneven batches, SpMV variants + a large solve, serving.
+# ---------------------------------------------------------------------------
+def _ev_ms(torch, fn, stream, reps, flush=None):
+    """Device time of fn(), L2 flushed before each rep.  A
+    short device-side spin before the start event keeps the host's launch
+    overhead out of the timed interval; one untimed call first (module
+    loading, first-touch allocations).  Median of the reps."""
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for i in range(reps):
+        with torch.cuda.stream(stream):
+            torch.cuda._sleep(HOST_AHEAD_CYCLES)
+            if flush is not None:
+                flush.fill_(float(i))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+def suite_uneven(torch, api, mna, oracle, stream, flush):
+    """512 analog matrices, n ~ U[100, 5000], distinct patterns, 8 Newton
+    refactors each: 4096 systems in one launch."""
+    rng = np.random.default_rng(42)
+    sizes = rng.integers(100, 5001, 512)
+    t0 = time.perf_counter()
+    mats = [mna.analog(int(n), 42 + i) for i, n in enumerate(sizes)]
+    pats = [api.Pattern.from_matrix(m) for m in mats]
+    t_an = time.perf_counter() - t0
+    vals, rhs, plist, owner = [], [], [], []
+    for i, m in enumerate(mats):
+        for v in m.perturbed(8, seed=1000 + i):
+            vals.append(v)
+            rhs.append(m.b)
+            plist.append(pats[i])
+            owner.append(i)
+    out = {"workload": "512 analog MNA matrices, n ~ U[100,5000], distinct patterns, 8 refactors each "
+                       "(4096 systems per launch)", "host_analysis_s_for_512_patterns": t_an}
+    sample = np.random.default_rng(7).choice(len(vals), 128, replace=False)
+    for prec, name in ((api.MIXED, "mixed"), (api.FP64, "fp64")):
+        B = api.Batch(plist, prec=prec)
+        B.upload(vals, rhs, stream=stream)
+        for _ in range(2):
+            B.run(api.RUN_BOTH, stream=stream, graph=True)
+        ms = _ev_ms(torch, lambda: B.run(api.RUN_BOTH, stream=stream, graph=True), stream, 3, flush)
+        xs = B.split(B.download(stream=stream))
+        torch.cuda.synchronize()
+        acc = 0
+        for s in sample:
+            m = mats[owner[s]]
+            _, q = plist[s].perm()
+            ref = oracle.ref_cpu_solve(m.n, m.Ap, m.Ai, vals[s], q, m.b)
+            acc += int(np.linalg.norm(xs[s] - ref) / np.linalg.norm(ref) <= 1e-6)
+        out[name] = {"ms_per_launch": ms, "systems_per_s": len(vals) / (ms / 1000.0),
+                     "accepted_in_sample": f"{acc}/{len(sample)}"}
+        B.close()
+    return out
+
+
+def suite_large(torch, api, mna, oracle, stream, flush, lib):
+    """n = 40,000 circuit with supply nets: SpMV variants (HBM GB/s vs the
+    measured peak) and a full mixed-precision GMRES-IR solve."""
+    import ctypes as C
+    hbm, kind = peaks()
+    m = mna.large_circuit()
+    A = m.csr()
+    n, nnz = m.n, A.nnz
+    x = np.random.default_rng(4).standard_normal(n)
+    dev = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a)).to(device="cuda", dtype=dt)
+    rp, ci = dev(A.indptr, torch.int32), dev(A.indices, torch.int32)
+    v64, v32 = dev(A.data, torch.float64), dev(A.data.astype(np.float32), torch.float32)
+    dx, dy = dev(x, torch.float64), torch.zeros(n, dtype=torch.float64, device="cuda")
+    p = lambda t: C.c_void_p(t.data_ptr())
+    st = C.c_void_p(stream.cuda_stream)
+    out = {"workload": f"large circuit n={n}, nnz={nnz}, "
+                       f"{100 * m.meta.get('frac_below_fp16_normal', 0):.0f}% of values below the fp16 normal minimum",
+           "peak_gbs": hbm, "peak_kind": kind}
+    spmv = {}
+
+    def rec(name, fn, sv):
+        ms = _ev_ms(torch, fn, stream, 20, flush)
+        b = nnz * (sv + 4) + (n + 1) * 4 + 16 * n
+        spmv[name] = {"us": ms * 1000.0, "GB_s": b / (ms / 1000.0) / 1e9, "frac": b / (ms / 1000.0) / 1e9 / hbm}
+
+    rec("csr_fp64", lambda: lib.spmv_launch(n, p(rp), p(ci), p(v64), p(dx), p(dy), st), 8)
+    rec("csr_fp32", lambda: lib.lusp_csr_spmv32(n, p(rp), p(ci), p(v32), p(dx), p(dy), st), 4)
+    for kind_, sv in (("fp64", 8), ("fp32", 4), ("fp16", 2)):
+        try:
+            S = api.Sell(n, A.indptr, A.indices, A.data, 32, 256, kind_)
+        except api.LuspError as e:
+            spmv[f"sell32_256_{kind_}"] = {"refused": str(e)}
+            continue
+        rec(f"sell32_256_{kind_}", lambda: S.spmv(dx.data_ptr(), dy.data_ptr(), stream=stream), sv)
+        spmv[f"sell32_256_{kind_}"]["padding"] = S.stored / max(S.nnz, 1)
+        S.close()
+    out["spmv"] = spmv
+    t0 = time.perf_counter()
+    P = api.Pattern.from_matrix(m)
+    out["host_analysis_s"] = time.perf_counter() - t0
+    _, q = P.perm()
+    ref = oracle.ref_cpu_solve(n, m.Ap, m.Ai, m.Ax, q, m.b)
+    for prec, inner, name in ((api.MIXED, 1, "mixed_inner_fp64"), (api.FP64, 0, "fp64")):
+        B = api.Batch([P], prec=prec, inner_prec=inner, max_outer=10)
+        B.upload([m.Ax], [m.b], stream=stream)
+        B.run(api.RUN_BOTH, stream=stream)
+        ms = _ev_ms(torch, lambda: B.run(api.RUN_BOTH, stream=stream), stream, 3, flush)
+        xg = B.download(stream=stream)
+        torch.cuda.synchronize()
+        stt = B.stats(stream=stream)[0]
+        out[name] = {"refactor_solve_ms": ms, "rel_err": float(np.linalg.norm(xg - ref) / np.linalg.norm(ref)),
+                     "status": stt["status"], "outer": stt["outer_iters"], "inner": stt["inner_iters"],
+                     "dense_tail": P.info["dense_tail"]}
+        B.close()
+    return out
+
+
+def suite_serving(torch, api, mna, oracle, stream):
+    """Poisson request stream over pattern classes through the serving loop:
+    90% fresh values on a cached pattern, 10% a new pattern, 5% ill-conditioned
+    (one subcircuit's conductances scaled to 1e-14); p50/p99 latency and
+    throughput vs plain per-request fp64 GPU solves."""
+    rng = np.random.default_rng(42)
+    sizes = np.exp(rng.uniform(np.log(113), np.log(8000), 16)).astype(int)
+    classes = [mna.analog(int(n), 700 + i) for i, n in enumerate(sizes)]
+    nreq = 400
+    new_id = [0]
+
+    def make_requests(salt):
+        reqs = []
+        for r in range(nreq):
+            u = rng.random()
+            if u < 0.10:
+                m = mna.analog(int(rng.choice(sizes)), 5000 + new_id[0])
+                new_id[0] += 1
+                v = m.Ax
+            else:
+                m = classes[int(rng.integers(len(classes)))]
+                v = m.perturbed(1, seed=salt + r)[0]
+                if rng.random() < 0.05:
+                    v = mna.ill_conditioned(m, seed=salt + r)
+            reqs.append((m, v))
+        return reqs
+    out = {"workload": f"{nreq} requests over 16 analog pattern classes (n log-uniform [113, 8000]); 10% new "
+                       "patterns, 5% ill-conditioned; Poisson arrivals"}
+    S = api.Server(max_batch=64, streams=3, arena_gb=2.0, staging_mb=256)
+    for m in classes:            # warm the pattern cache (the classes are known ahead)
+        S.poll(S.submit(m.n, m.Ap, m.Ai, m.Ax, m.b), 120000)
+    for rate in (2000.0, 10000.0):
+        reqs = make_requests(int(rate))      # fresh values and fresh new patterns per rate
+        gaps = rng.exponential(1.0 / rate, nreq)
+        ids = []
+        t0 = time.perf_counter()
+        tnext = t0
+        for (m, v), g in zip(reqs, gaps):
+            tnext += g
+            while time.perf_counter() < tnext:
+                pass
+            ids.append(S.submit(m.n, m.Ap, m.Ai, v, m.b))
+        res = [S.poll(i, 300000) for i in ids]
+        span = time.perf_counter() - t0
+        lat = [r[1]["latency_ms"] for r in res]
+        ok = sum(int(r[1]["rc"] == 0) for r in res)
+        esc = sum(int(r[1]["escalated"]) for r in res)
+        acc, chk = 0, 0
+        for (m, v), r in list(zip(reqs, res))[:: max(1, nreq // 40)]:
+            ref = oracle.ref_cpu_solve(m.n, m.Ap, m.Ai, v, api.colamd(m.n, m.Ap, m.Ai), m.b)
+            if ref is None:
+                continue
+            chk += 1
+            acc += int(np.linalg.norm(r[0] - ref) / np.linalg.norm(ref) <= 1e-6)
+        out[f"rate_{int(rate)}_per_s"] = {"p50_ms": float(np.percentile(lat, 50)),
+                                          "p99_ms": float(np.percentile(lat, 99)),
+                                          "throughput_per_s": nreq / span, "completed_ok": ok,
+                                          "escalated": esc, "accepted_in_sample": f"{acc}/{chk}",
+                                          "mean_batch": float(np.mean([r[1]["batch_size"] for r in res]))}
+    out["server_stats"] = S.stats()
+    S.close()
+    # Plain per-request fp64 GPU solves of the same requests (patterns analysed beforehand).
+    pat_cache = {}
+    times = []
+    for m, v in reqs[:100]:
+        key = id(m)
+        if key not in pat_cache:
+            pat_cache[key] = api.Pattern.from_matrix(m)
+        B = api.Batch([pat_cache[key]], prec=api.FP64)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        B.upload([v], [m.b], stream=stream)
+        B.run(api.RUN_BOTH, stream=stream)
+        B.download(stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+        B.close()
+    out["fp64_per_request"] = {"mean_ms": statistics.mean(times), "per_s": 1000.0 / statistics.mean(times),
+                               "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99))}
+    return out
+
+
+def run_suite(args):
+    import torch
+    torch.cuda.set_device(0)
+    from luspice_b200 import _lib as L, api, mna
+    from oracle import oracle
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    parts = {"uneven": lambda: suite_uneven(torch, api, mna, oracle, stream, flush),
+             "large": lambda: suite_large(torch, api, mna, oracle, stream, flush, L.load()),
+             "serving": lambda: suite_serving(torch, api, mna, oracle, stream)}
+    for name in args.suite.split(","):
+        print(json.dumps({"suite": name, **parts[name]()}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -221,7 +443,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--suite", default="", help="comma list of uneven,large,serving: the other "
+                    "workloads, one JSON line each, instead of the default run")
     args = ap.parse_args()
+    if args.suite:
+        run_suite(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -255,6 +482,7 @@ def main():
         t0 = time.perf_counter()
         for i in range(args.steps):
             with torch.cuda.stream(stream):
+                torch.cuda._sleep(HOST_AHEAD_CYCLES)
                 flush.fill_(float(i))
                 ev[i][0].record(stream)
             step(B)
@@ -290,6 +518,7 @@ def main():
         B.run(api.RUN_REFACTOR, stream=stream)
         a, bq = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
+            torch.cuda._sleep(HOST_AHEAD_CYCLES)
             flush.fill_(float(i))
             a.record(stream)
         B.run(api.RUN_SOLVE, stream=stream)

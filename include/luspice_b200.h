@@ -222,6 +222,7 @@ typedef struct {
     double arena_gb;               /* device arena per stream (default 2) */
     double staging_mb;             /* pinned host staging per stream (default 256) */
     int escalate;                  /* re-run failed mixed systems in fp64 (default 1) */
+    int analysis_threads;          /* host threads analysing new patterns (default 4) */
 } lusp_server_opts;
 
 typedef struct {
@@ -264,7 +265,10 @@ typedef struct lusp_sell lusp_sell;
 /* Build from a 0-based CSR: C in {8,16,32}, sigma >= C (row sort window),
  * value storage 0 = fp64, 1 = fp32, 2 = fp16 with Ruiz scaling (values are
  * stored as D_r A D_c in fp16, y = D_r^-1 (S (D_c^-1 x)); creation fails
- * with LUSP_EARG when a scaled value is outside the fp16 normal range). */
+ * with LUSP_EARG when a scaled value is outside the fp16 normal range).
+ * Rows longer than max(256, 8 x the mean row length) are kept out of the
+ * slices (one would set its whole slice's width) and computed in the same
+ * launch by a warp each; `stored` counts slice slots plus their entries. */
 int lusp_sell_create(int n, const int *rowptr, const int *colidx, const double *vals,
                      int C, int sigma, int value_kind, lusp_sell **out);
 void lusp_sell_destroy(lusp_sell *s);

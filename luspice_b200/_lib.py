@@ -48,7 +48,7 @@ class BatchOpts(C.Structure):
 class ServerOpts(C.Structure):
     _fields_ = [("solver", BatchOpts), ("max_batch", C.c_int), ("streams", C.c_int),
                 ("hbm_budget_gb", C.c_double), ("arena_gb", C.c_double), ("staging_mb", C.c_double),
-                ("escalate", C.c_int)]
+                ("escalate", C.c_int), ("analysis_threads", C.c_int)]
 
 
 class ServeResult(C.Structure):

@@ -1134,11 +1134,22 @@ __device__ void cta_spmv(const PatternDev& P, const AT* vals, const double* xin,
     for (int s = warp; s < P.nslices; s += nw) {
         const int base = P.sell_ptr[s];
         const int L = (P.sell_ptr[s + 1] - base) >> 5;
-        double acc = 0.0;
-        for (int t = 0; t < L; t++) {
+        // Four independent partial sums: four loads per lane in flight.
+        double acc = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int t = 0;
+        for (; t + 3 < L; t += 4) {
+            const int e = base + (t << 5) + lane;
+            const int c0 = P.sell_col[e], c1 = P.sell_col[e + 32], c2 = P.sell_col[e + 64], c3 = P.sell_col[e + 96];
+            acc = fma((double)vals[e], xin[c0], acc);
+            a1 = fma((double)vals[e + 32], xin[c1], a1);
+            a2 = fma((double)vals[e + 64], xin[c2], a2);
+            a3 = fma((double)vals[e + 96], xin[c3], a3);
+        }
+        for (; t < L; t++) {
             const int e = base + (t << 5) + lane;
             acc = fma((double)vals[e], xin[P.sell_col[e]], acc);
         }
+        acc = (acc + a1) + (a2 + a3);
         const int row = P.sell_perm[(s << 5) + lane];
         if (row >= 0) out[row] = RESID ? bt[row] - acc : acc;
     }

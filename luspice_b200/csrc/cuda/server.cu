@@ -1,8 +1,10 @@
 // Serving loop: continuous batching of refactor+solve requests.
 //
-// Threads: callers (submit / poll), one analysis thread (host COLAMD +
-// pivoting factorization of new patterns, then the device upload), one
-// scheduler thread (launches and completions).  Each stream owns a device
+// Threads: callers (submit / poll), analysis threads (host COLAMD +
+// pivoting factorization of new patterns, then the device upload; several
+// new patterns are analysed at once), one scheduler thread (launches and
+// completions).  The server's threads work on the device that was current
+// when it was created.  Each stream owns a device
 // arena and a pinned staging area; a launch bump-allocates all of its
 // systems in the arena, so nothing is allocated on the device per request.
 #include <cuda_runtime.h>
@@ -95,7 +97,9 @@ struct ServerObj {
     std::vector<Flight> flights;
     size_t pattern_bytes = 0, pattern_budget = 0;
     lusp_server_stats stats{};
-    std::thread sched, analysis;
+    std::thread sched;
+    std::vector<std::thread> analysis;               // host analysis of new patterns
+    int device = 0;                                  // the device the server was created on
 
     int init();
     void shutdown();
@@ -107,6 +111,7 @@ struct ServerObj {
 };
 
 int ServerObj::init() {
+    cudaGetDevice(&device);
     const int ns = std::max(1, opts.streams);
     flights.resize(ns);
     const size_t arena = (size_t)(opts.arena_gb * 1e9);
@@ -123,7 +128,8 @@ int ServerObj::init() {
     }
     const double budget = opts.hbm_budget_gb * 1e9 - (double)arena * ns;
     pattern_budget = budget > 0 ? (size_t)budget : 0;
-    analysis = std::thread([this] { analysis_loop(); });
+    const int na = opts.analysis_threads > 0 ? opts.analysis_threads : 4;
+    for (int t = 0; t < na; t++) analysis.emplace_back([this] { analysis_loop(); });
     sched = std::thread([this] { sched_loop(); });
     return LUSP_OK;
 }
@@ -143,7 +149,8 @@ void ServerObj::shutdown() {
     cv_sched.notify_all();
     cv_analysis.notify_all();
     if (sched.joinable()) sched.join();
-    if (analysis.joinable()) analysis.join();
+    for (auto& t : analysis)
+        if (t.joinable()) t.join();
     for (auto& f : flights) {
         if (f.st) cudaStreamSynchronize(f.st);
         if (f.arena) cudaFree(f.arena);
@@ -157,6 +164,7 @@ void ServerObj::shutdown() {
 }
 
 void ServerObj::analysis_loop() {
+    cudaSetDevice(device);
     while (true) {
         PatternEntry* pe = nullptr;
         {
@@ -458,6 +466,7 @@ void ServerObj::complete(Flight& f) {
 }
 
 void ServerObj::sched_loop() {
+    cudaSetDevice(device);
     std::unique_lock<std::mutex> lk(mu);
     while (true) {
         bool progress = false;
@@ -501,6 +510,7 @@ void lusp_server_opts_default(lusp_server_opts* o) {
     o->arena_gb = 2.0;
     o->staging_mb = 256.0;
     o->escalate = 1;
+    o->analysis_threads = 4;
 }
 
 int lusp_server_create(const lusp_server_opts* o, lusp_server** out) {

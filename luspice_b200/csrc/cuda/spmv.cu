@@ -36,9 +36,21 @@ csr_vector_kernel(int n, const int* __restrict__ rowptr, const int* __restrict__
     const int sub = threadIdx.x % kCsrLanes;
     double acc = 0.0;
     if (g < n) {
+        // Four independent partial sums keep four loads per lane in flight
+        // (long rows would otherwise wait one memory latency per entry).
         const int p1 = rowptr[g + 1];
-        for (int p = rowptr[g] + sub; p < p1; p += kCsrLanes)
-            acc = fma((double)values[p], __ldg(x + colidx[p]), acc);
+        double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int p = rowptr[g] + sub;
+        for (; p + 3 * kCsrLanes < p1; p += 4 * kCsrLanes) {
+            const int c0 = colidx[p], c1 = colidx[p + kCsrLanes], c2 = colidx[p + 2 * kCsrLanes],
+                      c3 = colidx[p + 3 * kCsrLanes];
+            acc = fma((double)values[p], __ldg(x + c0), acc);
+            a1 = fma((double)values[p + kCsrLanes], __ldg(x + c1), a1);
+            a2 = fma((double)values[p + 2 * kCsrLanes], __ldg(x + c2), a2);
+            a3 = fma((double)values[p + 3 * kCsrLanes], __ldg(x + c3), a3);
+        }
+        for (; p < p1; p += kCsrLanes) acc = fma((double)values[p], __ldg(x + colidx[p]), acc);
+        acc = (acc + a1) + (a2 + a3);
     }
 #pragma unroll
     for (int o = kCsrLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -52,12 +64,41 @@ template <> __device__ __forceinline__ double ldv<__half>(const __half* p) {
     return (double)__half2float(__ldg(p));
 }
 
+// Blocks [0, sell_blocks) take the slices; the blocks after them take the
+// long rows, a warp per row (lanes over its entries, four partial sums per
+// lane, a fixed-order warp reduction).
 template <int C, typename VT>
 __global__ void __launch_bounds__(256)
 sell_kernel(int nslices, const int* __restrict__ ptr, const int* __restrict__ col,
             const VT* __restrict__ val, const int* __restrict__ perm,
             const double* __restrict__ x, double* __restrict__ y,
-            const double* __restrict__ row_scale) {
+            const double* __restrict__ row_scale, int sell_blocks, int nlong,
+            const int* __restrict__ lrow, const int* __restrict__ lptr, const int* __restrict__ lcol,
+            const VT* __restrict__ lval) {
+    if ((int)blockIdx.x >= sell_blocks) {
+        const int lane = threadIdx.x & 31;
+        const int w = ((blockIdx.x - sell_blocks) * blockDim.x + threadIdx.x) >> 5;
+        if (w >= nlong) return;
+        const int p1 = lptr[w + 1];
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int p = lptr[w] + lane;
+        for (; p + 96 < p1; p += 128) {
+            const int c0 = lcol[p], c1 = lcol[p + 32], c2 = lcol[p + 64], c3 = lcol[p + 96];
+            a0 = fma(ldv<VT>(lval + p), __ldg(x + c0), a0);
+            a1 = fma(ldv<VT>(lval + p + 32), __ldg(x + c1), a1);
+            a2 = fma(ldv<VT>(lval + p + 64), __ldg(x + c2), a2);
+            a3 = fma(ldv<VT>(lval + p + 96), __ldg(x + c3), a3);
+        }
+        for (; p < p1; p += 32) a0 = fma(ldv<VT>(lval + p), __ldg(x + lcol[p]), a0);
+        double acc = (a0 + a1) + (a2 + a3);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+            const int row = lrow[w];
+            y[row] = row_scale ? acc * row_scale[row] : acc;
+        }
+        return;
+    }
     constexpr int G = 32 / C;
     const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (s >= nslices) return;
@@ -65,11 +106,21 @@ sell_kernel(int nslices, const int* __restrict__ ptr, const int* __restrict__ co
     const int r = lane % C, sub = lane / C;
     const int base = ptr[s];
     const int L = (ptr[s + 1] - base) / C;
-    double acc = 0.0;
-    for (int t = sub; t < L; t += G) {
+    double acc = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int t = sub;
+    for (; t + 3 * G < L; t += 4 * G) {
+        const int e = base + t * C + r, d = G * C;
+        const int c0 = col[e], c1 = col[e + d], c2 = col[e + 2 * d], c3 = col[e + 3 * d];
+        acc = fma(ldv<VT>(val + e), __ldg(x + c0), acc);
+        a1 = fma(ldv<VT>(val + e + d), __ldg(x + c1), a1);
+        a2 = fma(ldv<VT>(val + e + 2 * d), __ldg(x + c2), a2);
+        a3 = fma(ldv<VT>(val + e + 3 * d), __ldg(x + c3), a3);
+    }
+    for (; t < L; t += G) {
         const int e = base + t * C + r;
         acc = fma(ldv<VT>(val + e), __ldg(x + col[e]), acc);
     }
+    acc = (acc + a1) + (a2 + a3);
 #pragma unroll
     for (int o = 16; o >= C; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (sub == 0) {
@@ -97,6 +148,13 @@ struct SellObj {
     double* d_cs = nullptr;     // fp16: column scale
     double* d_xs = nullptr;     // fp16: scaled x
     double smin = 0, smax = 0;
+    // Rows much longer than the rest (supply nets) stay out of the slices
+    // (one of them would set a whole slice's width): CSR, a warp per row.
+    int nlong = 0;
+    int* d_lrow = nullptr;      // [nlong] row
+    int* d_lptr = nullptr;      // [nlong+1]
+    int* d_lcol = nullptr;
+    void* d_lval = nullptr;
 };
 
 // Ruiz equilibration (max norm): alternately scale rows and columns by
@@ -239,21 +297,25 @@ int lusp_sell_create(int n, const int* rowptr, const int* colidx, const double* 
                 return LUSP_EARG;
             }
         }
-        std::vector<int> len(n), perm(n);
+        std::vector<int> len(n), perm, lrows;
         for (int i = 0; i < n; i++) len[i] = rowptr[i + 1] - rowptr[i];
-        std::iota(perm.begin(), perm.end(), 0);
-        for (int w0 = 0; w0 < n; w0 += sigma) {
-            const int w1 = std::min(n, w0 + sigma);
+        // Rows longer than max(256, 8 x the mean row length) go to the long
+        // list; the rest are sorted by length inside windows of sigma rows.
+        const long thr = std::max<long>(256, 8 * ((rowptr[n] + n - 1) / n));
+        for (int i = 0; i < n; i++) (len[i] > thr ? lrows : perm).push_back(i);
+        const int nsh = (int)perm.size();
+        for (int w0 = 0; w0 < nsh; w0 += sigma) {
+            const int w1 = std::min(nsh, w0 + sigma);
             std::stable_sort(perm.begin() + w0, perm.begin() + w1, [&len](int a, int b) { return len[a] > len[b]; });
         }
-        const int ns = (n + C - 1) / C;
+        const int ns = (nsh + C - 1) / C;
         S->nslices = ns;
         std::vector<int> ptr(ns + 1, 0), hperm((size_t)ns * C, -1);
         for (int s = 0; s < ns; s++) {
             int ml = 0;
             for (int r = 0; r < C; r++) {
                 const int k = s * C + r;
-                if (k < n) { hperm[k] = perm[k]; ml = std::max(ml, len[perm[k]]); }
+                if (k < nsh) { hperm[k] = perm[k]; ml = std::max(ml, len[perm[k]]); }
             }
             ptr[s + 1] = ptr[s] + ml * C;
         }
@@ -264,7 +326,7 @@ int lusp_sell_create(int n, const int* rowptr, const int* colidx, const double* 
         for (int s = 0; s < ns; s++)
             for (int r = 0; r < C; r++) {
                 const int k = s * C + r;
-                if (k >= n) continue;
+                if (k >= nsh) continue;
                 const int row = perm[k];
                 const int L = (ptr[s + 1] - ptr[s]) / C;
                 for (int t = 0; t < L; t++) {
@@ -300,6 +362,41 @@ int lusp_sell_create(int n, const int* rowptr, const int* colidx, const double* 
                 e = cudaMemcpy(S->d_val, h.data(), h.size() * 2, cudaMemcpyHostToDevice);
             }
         }
+        // Long rows: CSR in their original order, values as stored above.
+        S->nlong = (int)lrows.size();
+        if (e == cudaSuccess && S->nlong > 0) {
+            std::vector<int> lptr(S->nlong + 1, 0), lcol;
+            std::vector<double> lv;
+            for (int t = 0; t < S->nlong; t++) {
+                const int row = lrows[t];
+                for (int p = rowptr[row]; p < rowptr[row + 1]; p++) {
+                    lcol.push_back(colidx[p]);
+                    lv.push_back(value_kind == 2 ? vals[p] * rs[row] * cs[colidx[p]] : vals[p]);
+                }
+                lptr[t + 1] = (int)lcol.size();
+            }
+            S->stored += (long)lcol.size();
+            e = cudaMalloc((void**)&S->d_lrow, lrows.size() * sizeof(int));
+            if (e == cudaSuccess) e = cudaMalloc((void**)&S->d_lptr, lptr.size() * sizeof(int));
+            if (e == cudaSuccess) e = cudaMalloc((void**)&S->d_lcol, lcol.size() * sizeof(int));
+            if (e == cudaSuccess) e = cudaMalloc(&S->d_lval, lv.size() * vsz);
+            if (e == cudaSuccess) e = cudaMemcpy(S->d_lrow, lrows.data(), lrows.size() * sizeof(int), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpy(S->d_lptr, lptr.data(), lptr.size() * sizeof(int), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpy(S->d_lcol, lcol.data(), lcol.size() * sizeof(int), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) {
+                if (value_kind == 0) {
+                    e = cudaMemcpy(S->d_lval, lv.data(), lv.size() * 8, cudaMemcpyHostToDevice);
+                } else if (value_kind == 1) {
+                    std::vector<float> f(lv.size());
+                    for (size_t t = 0; t < f.size(); t++) f[t] = (float)lv[t];
+                    e = cudaMemcpy(S->d_lval, f.data(), f.size() * 4, cudaMemcpyHostToDevice);
+                } else {
+                    std::vector<__half> h(lv.size());
+                    for (size_t t = 0; t < h.size(); t++) h[t] = __double2half(lv[t]);
+                    e = cudaMemcpy(S->d_lval, h.data(), h.size() * 2, cudaMemcpyHostToDevice);
+                }
+            }
+        }
         if (e == cudaSuccess && value_kind == 2) {
             std::vector<double> rinv(n);
             for (int i = 0; i < n; i++) rinv[i] = 1.0 / rs[i];
@@ -331,6 +428,10 @@ void lusp_sell_destroy(lusp_sell* hs) {
     cudaFree(S->d_rinv);
     cudaFree(S->d_cs);
     cudaFree(S->d_xs);
+    cudaFree(S->d_lrow);
+    cudaFree(S->d_lptr);
+    cudaFree(S->d_lcol);
+    cudaFree(S->d_lval);
     delete S;
 }
 
@@ -343,20 +444,24 @@ int lusp_sell_spmv(const lusp_sell* hs, const double* d_x, double* d_y, void* st
         scale_kernel<<<(S->n + 255) / 256, 256, 0, st>>>(S->n, d_x, S->d_cs, S->d_xs);
         xin = S->d_xs;
     }
-    const long threads = (long)S->nslices * 32;
-    const int grid = (int)((threads + 255) / 256);
+    const int sell_blocks = (int)(((long)S->nslices * 32 + 255) / 256);
+    const int long_blocks = (int)(((long)S->nlong * 32 + 255) / 256);
+    const int grid = sell_blocks + long_blocks;
     const double* rsc = S->kind == 2 ? S->d_rinv : nullptr;
 #define LUSP_SELL_CASE(CC)                                                                        \
     if (S->C == CC) {                                                                             \
         if (S->kind == 0)                                                                         \
             sell_kernel<CC, double><<<grid, 256, 0, st>>>(S->nslices, S->d_ptr, S->d_col,         \
-                (const double*)S->d_val, S->d_perm, xin, d_y, rsc);                               \
+                (const double*)S->d_val, S->d_perm, xin, d_y, rsc, sell_blocks, S->nlong,         \
+                S->d_lrow, S->d_lptr, S->d_lcol, (const double*)S->d_lval);                       \
         else if (S->kind == 1)                                                                    \
             sell_kernel<CC, float><<<grid, 256, 0, st>>>(S->nslices, S->d_ptr, S->d_col,          \
-                (const float*)S->d_val, S->d_perm, xin, d_y, rsc);                                \
+                (const float*)S->d_val, S->d_perm, xin, d_y, rsc, sell_blocks, S->nlong,          \
+                S->d_lrow, S->d_lptr, S->d_lcol, (const float*)S->d_lval);                        \
         else                                                                                      \
             sell_kernel<CC, __half><<<grid, 256, 0, st>>>(S->nslices, S->d_ptr, S->d_col,         \
-                (const __half*)S->d_val, S->d_perm, xin, d_y, rsc);                               \
+                (const __half*)S->d_val, S->d_perm, xin, d_y, rsc, sell_blocks, S->nlong,         \
+                S->d_lrow, S->d_lptr, S->d_lcol, (const __half*)S->d_lval);                       \
     }
     LUSP_SELL_CASE(8)
     LUSP_SELL_CASE(16)

@@ -127,3 +127,27 @@ def test_singular_flagged(gpu):
     st = B.stats()[0]
     assert st["status"] & api.ST_SINGULAR
     assert st["singular_col"] >= 0
+
+
+@pytest.mark.parametrize("prec", [api.MIXED, api.FP64])
+def test_cluster_refactor_bitwise(gpu, prec):
+    """One system's columns spread over a 2-CTA thread-block cluster give the
+    same factor bit for bit, and the same pivot statistics, as one CTA."""
+    m = mna.power_grid()
+    P = api.Pattern.from_matrix(m)
+    vals = m.perturbed(3, seed=21)
+    out = []
+    for rc in (1, 2):
+        B = api.Batch([P] * 3, prec=prec, refactor_cluster=rc)
+        B.upload(list(vals), [m.b] * 3)
+        B.run(api.RUN_REFACTOR)
+        out.append(([B.factor_values(s) for s in range(3)], B.stats()))
+        B.close()
+    for s in range(3):
+        exp, bad = oracle_refactor(m, P, vals[s], fp32=(prec == api.MIXED))
+        for f, _ in out:
+            got = f[s]
+            ity = np.uint32 if got.dtype == np.float32 else np.uint64
+            assert np.array_equal(got.view(ity), exp.astype(got.dtype).view(ity))
+        for k in ("min_abs_pivot", "min_pivot_ratio", "max_abs_u", "status", "singular_col"):
+            assert out[0][1][s][k] == out[1][1][s][k], k
