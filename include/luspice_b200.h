@@ -277,6 +277,22 @@ int lusp_sell_spmv(const lusp_sell *s, const double *d_x, double *d_y, void *str
 int lusp_sell_info(const lusp_sell *s, long *stored, long *nnz, double *fp16_scaled_min,
                    double *fp16_scaled_max);
 
+/* ---- autotuning (measured on this GPU) ---- */
+/* Times refactor + solve of nsys copies of (Ax, b) for candidate
+ * configurations — dense trailing block (none, the cost model's choice,
+ * half of it, larger), refactor cluster size (1, 2), solve-kernel CTA
+ * (256, 512 threads) and sweep kind (level-synchronous, dataflow) — and
+ * returns the fastest: *opts is updated (its other fields are kept),
+ * *dense_tail is the block size to pass to lusp_pattern_create_ex, and
+ * *best_ms the time of one launch.  Takes about a second per candidate
+ * block size for matrices of a few thousand rows. */
+int lusp_tune(int n, const int *Ap, const int *Ai, const double *Ax, const double *b, int nsys,
+              lusp_batch_opts *opts, int *dense_tail, double *best_ms);
+/* Fastest SELL slice height C in {8,16,32} and sort window sigma in
+ * {32,256,1024} for this CSR matrix and value storage (as lusp_sell_create). */
+int lusp_sell_tune(int n, const int *rowptr, const int *colidx, const double *vals, int value_kind,
+                   int *C, int *sigma, double *best_us);
+
 #ifdef __cplusplus
 }
 #endif

@@ -101,6 +101,10 @@ SIGNATURES = {
     "lusp_device_count": (C.c_int, []),
     "lusp_pattern_create": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, c_void_pp]),
     "lusp_pattern_create_ex": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, C.c_int, c_void_pp]),
+    "lusp_tune": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, c_double_p, C.c_int, C.c_void_p,
+                            C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "lusp_sell_tune": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, C.c_int, C.POINTER(C.c_int),
+                                 C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "lusp_pattern_destroy": (None, [C.c_void_p]),
     "lusp_pattern_get_info": (C.c_int, [C.c_void_p, C.POINTER(PatternInfo)]),
     "lusp_pattern_get_perm": (C.c_int, [C.c_void_p, c_int_p, c_int_p]),

@@ -323,3 +323,30 @@ def pivot_factor(n: int, Ap, Ai, Ax, q=None, tol: float = 1.0) -> dict:
     _check(lib.lusp_pivot_factor(*args(Li, Lx, Ui, Ux, cap)), "lusp_pivot_factor")
     return {"singular_col": -1, "pinv": pinv, "Lp": Lp, "Li": Li[:ln.value], "Lx": Lx[:ln.value],
             "Up": Up, "Ui": Ui[:un.value], "Ux": Ux[:un.value], "lnnz": ln.value, "unnz": un.value}
+
+
+def autotune(m, nsys: int, prec: int = MIXED, **opts) -> dict:
+    """Measure candidate configurations for nsys copies of matrix m (an
+    MNAMatrix-like object with n, Ap, Ai, Ax, b) on this GPU; returns the
+    fastest as {"dense_tail": D, "opts": {...}, "ms": t}: build the pattern
+    with Pattern(..., dense_tail=D) and the batch with **opts."""
+    lib = L.load()
+    o = default_opts()
+    o.prec = prec
+    for k, v in opts.items():
+        setattr(o, k, v)
+    Ap, Ai, Ax, b = _i32(m.Ap), _i32(m.Ai), _f64(m.Ax), _f64(m.b)
+    d, ms = C.c_int(), C.c_double()
+    _check(lib.lusp_tune(int(m.n), L.ptr(Ap, C.c_int), L.ptr(Ai, C.c_int), L.ptr(Ax, C.c_double),
+                         L.ptr(b, C.c_double), int(nsys), C.byref(o), C.byref(d), C.byref(ms)), "lusp_tune")
+    keys = ("refactor_cluster", "block_threads", "ctas_per_sm", "solve_sweep")
+    return {"dense_tail": d.value, "opts": {k: getattr(o, k) for k in keys}, "ms": ms.value}
+
+
+def sell_tune(n, rowptr, colidx, vals, kind: str = "fp32") -> dict:
+    """Fastest SELL (C, sigma) for this CSR matrix: {"C", "sigma", "us"}."""
+    rp, ci, v = _i32(rowptr), _i32(colidx), _f64(vals)
+    c, sg, us = C.c_int(), C.c_int(), C.c_double()
+    _check(L.load().lusp_sell_tune(int(n), L.ptr(rp, C.c_int), L.ptr(ci, C.c_int), L.ptr(v, C.c_double),
+                                   Sell.KINDS[kind], C.byref(c), C.byref(sg), C.byref(us)), "lusp_sell_tune")
+    return {"C": c.value, "sigma": sg.value, "us": us.value}
