@@ -110,8 +110,9 @@ def algorithmic_bytes(info, stats, vs=4):
       refactor  nnz(A)(8+4) + (n+1)4 + nnz(L+U)(vs+4) + 4n
       trisolve  nnz(L+U)(vs+4) + 2(n+1)4 + 3*8n
       SpMV      nnz(A)(s_v+4) + (n+1)4 + 8n + 8n
-      inner j   SpMV(vs) + trisolve + 2 passes (j+1) 2*8n
-      outer     SpMV(fp64) + 3*8n, plus one trisolve per correction."""
+      inner j   SpMV(vs) + trisolve + 2 passes (j+1) 2*8n + 8n (z_j kept)
+      outer     SpMV(fp64) + 3*8n; the correction sum_j y_j z_j reads the
+                kept z_j (8n each) and writes 8n."""
     n, nnz = info["n"], info["nnz_a"]
     lu = info["cap"]
     refactor = nnz * 12 + (n + 1) * 4 + lu * (vs + 4) + 4 * n
@@ -134,8 +135,8 @@ def algorithmic_bytes(info, stats, vs=4):
                 js.extend(range(c))
                 left -= c
             for j in js:
-                b += spmv_in + tri + 2 * (j + 1) * 2 * 8 * n
-            b += outer * tri
+                b += spmv_in + tri + 2 * (j + 1) * 2 * 8 * n + 8 * n
+            b += inner * 8 * n + outer * 8 * n
         total += b
     return total_ref, total
 
