@@ -50,7 +50,10 @@ enum {
     LUSP_ST_NONFINITE = 16,
     LUSP_ST_WAIT_TIMEOUT = 32,
     LUSP_ST_CAPACITY = 64,
-    LUSP_ST_ESCALATED = 128   /* result comes from the fp64 path */
+    LUSP_ST_ESCALATED = 128,  /* result comes from the fp64 path (server
+                                 re-queue, or a ladder rung) */
+    LUSP_ST_SHIFTED = 256,    /* ... from the ladder's P-hard rung */
+    LUSP_ST_LADDER_FULL = 512 /* the ladder had no slot left: P-fast result */
 };
 
 enum { LUSP_MIXED = 0, LUSP_FP64 = 1 };
@@ -79,7 +82,9 @@ typedef struct {
 typedef struct {
     double min_abs_pivot, min_pivot_ratio, max_abs_u;
     double res[16];                /* ||b - A x|| / ||b|| history */
-    int nres, inner_iters, outer_iters, status, singular_col, pad_;
+    int nres, inner_iters, outer_iters, status, singular_col;
+    int rung;                      /* what produced the result: 0 the batch's own
+                                      precision, 1 ladder P-safe, 2 ladder P-hard */
     /* SM cycles summed over warps: refactor waits for dependency columns,
      * gathers of their L parts, updates; refactor wall cycles of the CTA */
     long long cyc_wait, cyc_gather, cyc_update, cyc_refactor;
@@ -127,6 +132,21 @@ typedef struct {
                                       system's refactorization: 0 auto (2 when every
                                       system of the batch gets its own pair of SMs,
                                       else 1), or 1..8 */
+    int ladder;                    /* device-side escalation in the same launch, for a
+                                      LUSP_MIXED system whose solve fails (a status
+                                      failure bit, or a final residual above rtol):
+                                      0 off (default); 1 P-safe: refactor in fp64 and
+                                      solve by GMRES-IR with the fp64 factor; 2 P-hard:
+                                      the fp64 factor of A + hard_shift diag|A(i,i)|
+                                      (the residual still uses A); 3 P-safe, then
+                                      P-hard for the systems P-safe fails */
+    int ladder_slots;              /* systems the ladder takes per launch: 0 auto (all
+                                      systems up to 256, else max(256, nsys / 8)); a
+                                      failed system beyond them keeps its P-fast result
+                                      with LUSP_ST_LADDER_FULL */
+    double factor_shift;           /* factor A + factor_shift diag|A(i,i)| instead of A
+                                      (the residual still uses A; default 0) */
+    double hard_shift;             /* the P-hard rung's shift (default 1e-7) */
 } lusp_batch_opts;
 
 /* ---- library ---- */
@@ -194,8 +214,9 @@ int lusp_batch_factor_values(lusp_batch *b, int sys, void *out, void *stream);
 int lusp_batch_copy_values(lusp_batch *dst, const lusp_batch *src, void *stream);
 /* Device pointer to the merged factor values of one system. */
 int lusp_batch_factor_device_ptr(lusp_batch *b, int sys, void **d_values);
-/* Update max_outer, rtol, inner_rel, stag_ratio and pivot_tol (prec,
- * krylov and the launch shape are fixed at creation). */
+/* Update max_outer, rtol, inner_rel, stag_ratio, pivot_tol, xtol,
+ * factor_shift and hard_shift, for the ladder's rungs too (prec, krylov,
+ * ladder, ladder_slots and the launch shape are fixed at creation). */
 int lusp_batch_set_params(lusp_batch *b, const lusp_batch_opts *opts);
 /* Kernel launches issued by the last lusp_batch_run (for accounting). */
 int lusp_batch_launch_count(const lusp_batch *b);
@@ -210,8 +231,9 @@ int lusp_batch_launch_count(const lusp_batch *b);
  * separate host thread and kept on the device in an LRU cache keyed by a
  * hash of (n, Ap, Ai), within hbm_budget_gb together with the launch arenas.
  * A system whose mixed-precision solve fails (IR stagnation, no
- * convergence, non-finite, weak or zero pivot) is re-queued once on the
- * plain fp64 GPU path (LUSP_ST_ESCALATED in its result).  Results do not
+ * convergence, non-finite, weak or zero pivot) is escalated to fp64 as
+ * `escalate` says: on the device in the same launch, or re-queued once on
+ * the plain fp64 GPU path (LUSP_ST_ESCALATED in its result either way).  Results do not
  * depend on what else is in the launch (one CTA runs each system the same
  * way). */
 typedef struct {
@@ -221,7 +243,12 @@ typedef struct {
     double hbm_budget_gb;          /* pattern cache + arenas (default 150) */
     double arena_gb;               /* device arena per stream (default 2) */
     double staging_mb;             /* pinned host staging per stream (default 256) */
-    int escalate;                  /* re-run failed mixed systems in fp64 (default 1) */
+    int escalate;                  /* failed mixed systems: 0 kept as they are; 1 (default)
+                                      the device ladder's P-safe rung in the same launch
+                                      (lusp_batch_opts.ladder), and a system the ladder
+                                      had no slot for re-queued once on the plain fp64
+                                      path; 2 as 1 with P-safe then P-hard; 3 only the
+                                      re-queue on the plain fp64 path */
     int analysis_threads;          /* host threads analysing new patterns (default 4) */
 } lusp_server_opts;
 

@@ -28,7 +28,7 @@ class SysStats(C.Structure):
     _fields_ = [("min_abs_pivot", C.c_double), ("min_pivot_ratio", C.c_double),
                 ("max_abs_u", C.c_double), ("res", C.c_double * 16), ("nres", C.c_int),
                 ("inner_iters", C.c_int), ("outer_iters", C.c_int), ("status", C.c_int),
-                ("singular_col", C.c_int), ("pad_", C.c_int), ("cyc_wait", C.c_longlong),
+                ("singular_col", C.c_int), ("rung", C.c_int), ("cyc_wait", C.c_longlong),
                 ("cyc_gather", C.c_longlong), ("cyc_update", C.c_longlong), ("cyc_refactor", C.c_longlong),
                 ("cyc_lsolve", C.c_longlong), ("cyc_tail", C.c_longlong), ("cyc_usolve", C.c_longlong),
                 ("cyc_spmv", C.c_longlong), ("cyc_solve", C.c_longlong), ("cyc_tpanel", C.c_longlong),
@@ -42,7 +42,8 @@ class BatchOpts(C.Structure):
                 ("pivot_tol", C.c_double), ("block_threads", C.c_int), ("ctas_per_sm", C.c_int),
                 ("solve_sweep", C.c_int), ("refactor_mode", C.c_int), ("inner_prec", C.c_int),
                 ("xtol", C.c_double), ("refactor_threads", C.c_int),
-                ("refactor_cluster", C.c_int)]
+                ("refactor_cluster", C.c_int), ("ladder", C.c_int), ("ladder_slots", C.c_int),
+                ("factor_shift", C.c_double), ("hard_shift", C.c_double)]
 
 
 class ServerOpts(C.Structure):

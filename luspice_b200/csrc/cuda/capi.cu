@@ -162,6 +162,10 @@ void lusp_batch_opts_default(lusp_batch_opts* o) {
     o->xtol = 1e-8;
     o->refactor_threads = 0;
     o->refactor_cluster = 0;
+    o->ladder = 0;
+    o->ladder_slots = 0;
+    o->factor_shift = 0.0;
+    o->hard_shift = 1e-7;
 }
 
 int lusp_batch_create(int nsys, lusp_pattern* const* pats, const lusp_batch_opts* opts,
@@ -302,7 +306,16 @@ int lusp_batch_set_params(lusp_batch* hb, const lusp_batch_opts* o) {
     B->prm.stag_ratio = o->stag_ratio;
     B->prm.pivot_tol = o->pivot_tol;
     B->prm.xtol = o->xtol > 0 ? o->xtol : 1e-8;
+    if (o->factor_shift >= 0.0) B->prm.shift = o->factor_shift;
     B->launch.prm = B->prm;
+    if (B->launch.rungs) {
+        lusp::SolveParams& x = B->launch.xprm;
+        const double keep_shift = x.shift;
+        x = B->prm;
+        x.shift = keep_shift;
+        B->launch.esc.rtol = o->rtol;
+        if (o->hard_shift > 0) B->launch.hard_shift = o->hard_shift;
+    }
     // Captured graphs hold the old parameters by value.
     for (auto& kv : B->graphs) {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);

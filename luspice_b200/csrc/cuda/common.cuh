@@ -17,6 +17,9 @@ enum : int {
     ST_NONFINITE = 16,     // NaN/Inf in a residual
     ST_WAIT_TIMEOUT = 32,  // a bounded wait gave up (never expected)
     ST_CAPACITY = 64,      // a work area was too small (never expected)
+    ST_ESCALATED = 128,    // the result comes from an fp64 rung of the ladder
+    ST_SHIFTED = 256,      // ... from the P-hard rung (factor of A + shift diag|A|)
+    ST_LADDER_FULL = 512,  // the ladder had no free slot: P-fast result kept
 };
 
 // Spin bound for waits on shared-memory ready bits inside one CTA: about a

@@ -51,11 +51,20 @@ int cuda_fail(cudaError_t e, const char* what) {
 // queue[0] feeds the refactor kernel, queue[1] the solve kernel, queue[2]
 // the dense kernel.
 // ---------------------------------------------------------------------------
+// dyn (may be null): the number of systems is min(*dyn, nsys), set by an
+// earlier kernel of the launch; list (may be null): work item t is system
+// list[t] (the escalation ladder's slots).
+__device__ __forceinline__ int item_count(int nsys, const int* dyn) {
+    return dyn ? min(*(const volatile int*)dyn, nsys) : nsys;
+}
+
 template <typename VT>
 __global__ void __launch_bounds__(1024, 1)
-refactor_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan, SolveParams prm) {
+refactor_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan, SolveParams prm,
+                const int* dyn, const int* list) {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_task;
+    const int ns = item_count(nsys, dyn);
     // A thread-block cluster (or a lone CTA) takes one system at a time:
     // rank 0 draws it, every CTA reads it through distributed shared memory
     // between two cluster barriers (so rank 0 outlives the read).
@@ -68,41 +77,81 @@ refactor_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan p
         cl.sync();
         const int t = *task0;
         cl.sync();
-        if (t >= nsys) break;
-        const SysDev S = sys[t];
+        if (t >= ns) break;
+        const SysDev S = sys[list ? list[t] : t];
         refactor_phase<VT>(S, plan, smem, prm);
     }
 }
 
 template <typename VT>
 __global__ void __launch_bounds__(512, 1)
-dense_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan, SolveParams prm) {
+dense_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan, SolveParams prm,
+             const int* dyn, const int* list) {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_task;
+    const int ns = item_count(nsys, dyn);
     while (true) {
         __syncthreads();
         if (threadIdx.x == 0) s_task = atomicAdd(queue + 2, 1);
         __syncthreads();
         const int t = s_task;
-        if (t >= nsys) break;
-        const SysDev S = sys[t];
+        if (t >= ns) break;
+        const SysDev S = sys[list ? list[t] : t];
         dense_phase<VT>(S, plan, smem, prm);
+    }
+}
+
+// After the solve of one system (thread 0, past the CTA barrier that makes
+// the solve's statistics visible): record the rung that produced the
+// result and hand a failed system to the next rung of the ladder.
+__device__ void ladder_handoff(const SysDev& S, int item, const EscDev& esc, int rung) {
+    SysStats* st = S.stats;
+    st->rung = rung;
+    if (rung > 0) st->status |= ST_ESCALATED | (rung == 2 ? ST_SHIFTED : 0);
+    if (esc.cap <= 0 || rung == 2) return;
+    const int nres = st->nres;
+    const double last = nres > 0 ? st->res[nres - 1] : INFINITY;
+    const int bits = rung == 0 ? esc.fail_bits : (esc.fail_bits & ~ST_PIVOT_WEAK);
+    const bool failed = (st->status & bits) != 0 || !(last <= esc.rtol);
+    if (!failed) return;
+    if (rung == 0) {
+        // Storage first (a refused reservation takes no slot), then a slot.
+        const SysSizes z = sizes_of(*S.pat);
+        const size_t need = sys_private_bytes(z, sizeof(double), esc.m);
+        const unsigned long long off = atomicAdd((unsigned long long*)(esc.ctl + 2), (unsigned long long)need);
+        if (off + need > esc.pool) {
+            st->status |= ST_LADDER_FULL;
+            return;
+        }
+        const int slot = atomicAdd(&esc.ctl[0], 1);
+        if (slot >= esc.cap) {
+            st->status |= ST_LADDER_FULL;
+            return;
+        }
+        SysDev D = S;
+        sys_carve(D, esc.base + off, z, sizeof(double), esc.m);
+        D.scratch = esc.scratch;
+        esc.slots[slot] = D;
+    } else if (esc.hard) {
+        esc.hard[atomicAdd(&esc.ctl[1], 1)] = item;
     }
 }
 
 template <typename VT, typename AT>
 __global__ void __launch_bounds__(512)
 solve_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan,
-             SolveParams prm, int direct) {
+             SolveParams prm, int direct, const int* dyn, const int* list, EscDev esc, int rung) {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_task;
+    const int ns = item_count(nsys, dyn);
     while (true) {
         __syncthreads();
         if (threadIdx.x == 0) s_task = atomicAdd(queue + 1, 1);
         __syncthreads();
         const int t = s_task;
-        if (t >= nsys) break;
-        const SysDev S = sys[t];
+        if (t >= ns) break;
+        const int item = list ? list[t] : t;
+        const SysDev S = sys[item];
         const long long ts = clock64();
         if (threadIdx.x == 0) {
             S.stats->cyc_lsolve = 0;
@@ -116,7 +165,10 @@ solve_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan
         if (direct) direct_phase<VT>(S, plan, smem);
         else gmres_phase<VT, AT>(S, plan, smem, prm);
         __syncthreads();
-        if (threadIdx.x == 0) S.stats->cyc_solve = clock64() - ts;
+        if (threadIdx.x == 0) {
+            S.stats->cyc_solve = clock64() - ts;
+            ladder_handoff(S, item, esc, rung);
+        }
     }
 }
 
@@ -189,7 +241,7 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
                                         &S.lrp, &S.lci, &S.urp, &S.uci, &S.slot_dst, &S.fwd_order,
                                         &S.bwd_order, &S.sell_ptr, &S.sell_col, &S.sell_src,
                                         &S.sell_perm, &S.rowat, &S.q, &S.fwd_lev, &S.bwd_lev, &S.bwd_pos,
-                                        &S.fwd_ldesc, &S.bwd_ldesc, &S.dep_bc};
+                                        &S.fwd_ldesc, &S.bwd_ldesc, &S.dep_bc, &S.a_diag};
     const int narr = (int)(sizeof(arrays) / sizeof(arrays[0]));
     std::vector<size_t> off(narr + 1, 0);
     // Each array gets at least 8 ints of slack: the sweeps copy index runs
@@ -240,6 +292,7 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     D.fwd_ldesc = blk + off[idx++];
     D.bwd_ldesc = blk + off[idx++];
     D.dep_bc = (const int2*)(blk + off[idx++]);
+    D.a_diag = blk + off[idx++];
     D.lev_max_ent = S.lev_max_ent;
     D.lev_max_rows = S.lev_max_rows;
     D.nfwd_levels = S.nfwd_levels;
@@ -485,51 +538,98 @@ int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ) {
     return kernel_prepare<float, float>(smem, block, occ);
 }
 
+// Launch shapes of the three kernels of one rung.
+struct RungShape {
+    SmemPlan rplan, dplan, plan;
+    int rblock, rgrid, rcluster, dblock, dgrid, block, grid;
+};
+
+static RungShape main_shape(const LaunchArgs& a) {
+    return RungShape{a.rplan, a.dplan, a.plan, a.rblock, a.rgrid, a.rcluster, a.dblock, a.dgrid, a.block, a.grid};
+}
+
+static RungShape ladder_shape(const LaunchArgs& a) {
+    return RungShape{a.xrplan, a.xdplan, a.xplan, a.xrblock, a.xrgrid, a.xrcluster, a.xdblock, a.xdgrid,
+                     a.xblock, a.xgrid};
+}
+
+// Refactor, dense-block and solve kernels of one rung over sys[0, nsys) (or
+// the dyn / list items) with the work counters q[0..2].
 template <typename VT, typename AT>
-static int launch_typed(const LaunchArgs& a, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(a.d_queue, 0, 3 * sizeof(int), st);
-    if (e != cudaSuccess) return cuda_fail(e, "queue reset");
-    if (a.what & LUSP_RUN_REFACTOR) {
-        int rc = refactor_prepare<VT>(a.rplan.bytes, a.rblock, nullptr);
+static int launch_rung(const SysDev* sys, int nsys, int* q, const int* dyn, const int* list, int what,
+                       const RungShape& r, const SolveParams& prm, int direct, const EscDev& esc, int rung,
+                       cudaStream_t st) {
+    cudaError_t e;
+    if (what & LUSP_RUN_REFACTOR) {
+        int rc = refactor_prepare<VT>(r.rplan.bytes, r.rblock, nullptr);
         if (rc != LUSP_OK) return rc;
-        if (a.rcluster > 1) {
+        if (r.rcluster > 1) {
             cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3((unsigned)a.rgrid);
-            cfg.blockDim = dim3((unsigned)a.rblock);
-            cfg.dynamicSmemBytes = a.rplan.bytes;
+            cfg.gridDim = dim3((unsigned)r.rgrid);
+            cfg.blockDim = dim3((unsigned)r.rblock);
+            cfg.dynamicSmemBytes = r.rplan.bytes;
             cfg.stream = st;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeClusterDimension;
-            attr[0].val.clusterDim.x = (unsigned)a.rcluster;
+            attr[0].val.clusterDim.x = (unsigned)r.rcluster;
             attr[0].val.clusterDim.y = 1;
             attr[0].val.clusterDim.z = 1;
             cfg.attrs = attr;
             cfg.numAttrs = 1;
-            e = cudaLaunchKernelEx(&cfg, refactor_kernel<VT>, a.d_sys, a.nsys, a.d_queue, a.rplan, a.prm);
+            e = cudaLaunchKernelEx(&cfg, refactor_kernel<VT>, sys, nsys, q, r.rplan, prm, dyn, list);
         } else {
-            refactor_kernel<VT><<<a.rgrid, a.rblock, a.rplan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.rplan,
-                                                                          a.prm);
+            refactor_kernel<VT><<<r.rgrid, r.rblock, r.rplan.bytes, st>>>(sys, nsys, q, r.rplan, prm, dyn, list);
             e = cudaGetLastError();
         }
         if (e != cudaSuccess) return cuda_fail(e, "refactor kernel launch");
-        if (a.dgrid > 0) {
-            rc = dense_prepare<VT>(a.dplan.bytes, a.dblock, nullptr);
+        if (r.dgrid > 0) {
+            rc = dense_prepare<VT>(r.dplan.bytes, r.dblock, nullptr);
             if (rc != LUSP_OK) return rc;
-            dense_kernel<VT><<<a.dgrid, a.dblock, a.dplan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.dplan, a.prm);
+            dense_kernel<VT><<<r.dgrid, r.dblock, r.dplan.bytes, st>>>(sys, nsys, q, r.dplan, prm, dyn, list);
             e = cudaGetLastError();
             if (e != cudaSuccess) return cuda_fail(e, "dense kernel launch");
         }
     }
-    if (a.what & LUSP_RUN_SOLVE) {
-        int rc = kernel_prepare<VT, AT>(a.plan.bytes, a.block, nullptr);
+    if (what & LUSP_RUN_SOLVE) {
+        int rc = kernel_prepare<VT, AT>(r.plan.bytes, r.block, nullptr);
         if (rc != LUSP_OK) return rc;
-        const int direct = (a.prec == LUSP_FP64 || (a.what & LUSP_RUN_DIRECT)) ? 1 : 0;
-        solve_kernel<VT, AT><<<a.grid, a.block, a.plan.bytes, st>>>(a.d_sys, a.nsys, a.d_queue, a.plan, a.prm,
-                                                                  direct);
+        solve_kernel<VT, AT><<<r.grid, r.block, r.plan.bytes, st>>>(sys, nsys, q, r.plan, prm, direct, dyn, list,
+                                                                  esc, rung);
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "solve kernel launch");
     }
     return LUSP_OK;
+}
+
+template <typename VT, typename AT>
+static int launch_typed(const LaunchArgs& a, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(a.d_queue, 0, kQueueWords * sizeof(int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "queue reset");
+    const int direct = (a.prec == LUSP_FP64 || (a.what & LUSP_RUN_DIRECT)) ? 1 : 0;
+    const bool ladder = a.rungs != 0 && !direct && (a.what & LUSP_RUN_SOLVE);
+    EscDev none{};
+    int rc = launch_rung<VT, AT>(a.d_sys, a.nsys, a.d_queue, nullptr, nullptr, a.what, main_shape(a), a.prm, direct,
+                                 ladder ? a.esc : none, 0, st);
+    if (rc != LUSP_OK || !ladder) return rc;
+    // The fp64 rungs: every kernel reads its item count from the slot
+    // counters the solve kernels above wrote (no host round trip).
+    const RungShape x = ladder_shape(a);
+    int* ctl = a.d_queue + kLadderCtl;
+    if (a.rungs & 1) {
+        EscDev esc = a.esc;
+        if (!(a.rungs & 2)) esc.hard = nullptr;
+        rc = launch_rung<double, double>(a.esc.slots, a.esc.cap, a.d_queue + 3, ctl, nullptr, LUSP_RUN_BOTH, x,
+                                         a.xprm, 0, esc, 1, st);
+        if (rc != LUSP_OK) return rc;
+    }
+    if (a.rungs & 2) {
+        SolveParams hp = a.xprm;
+        hp.shift = a.hard_shift;
+        const bool after_safe = (a.rungs & 1) != 0;
+        rc = launch_rung<double, double>(a.esc.slots, a.esc.cap, a.d_queue + 6, after_safe ? ctl + 1 : ctl,
+                                         after_safe ? a.esc.hard : nullptr, LUSP_RUN_BOTH, x, hp, 0, a.esc, 2, st);
+    }
+    return rc;
 }
 
 int launch_systems(const LaunchArgs& a, cudaStream_t st) {
@@ -539,7 +639,11 @@ int launch_systems(const LaunchArgs& a, cudaStream_t st) {
 }
 
 int launch_kernel_count(const LaunchArgs& a, int what) {
-    return ((what & LUSP_RUN_REFACTOR) ? (a.dgrid > 0 ? 2 : 1) : 0) + ((what & LUSP_RUN_SOLVE) ? 1 : 0);
+    int n = ((what & LUSP_RUN_REFACTOR) ? (a.dgrid > 0 ? 2 : 1) : 0) + ((what & LUSP_RUN_SOLVE) ? 1 : 0);
+    const bool direct = a.prec == LUSP_FP64 || (what & LUSP_RUN_DIRECT);
+    if (a.rungs && !direct && (what & LUSP_RUN_SOLVE))
+        n += (((a.rungs & 1) ? 1 : 0) + ((a.rungs & 2) ? 1 : 0)) * (a.xdgrid > 0 ? 3 : 2);
+    return n;
 }
 
 int batch_launch(BatchObj* B, int what, cudaStream_t st) {
@@ -550,35 +654,19 @@ int batch_launch(BatchObj* B, int what, cudaStream_t st) {
     return rc;
 }
 
-static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
-
 int tail_ld(const StaticPattern& S) { return (S.dtail + 31) & ~31; }
 
+static SysSizes host_sizes(const StaticPattern& S) {
+    return SysSizes{(size_t)S.n, (size_t)S.cap, S.lci.size(), S.uci.size(), (size_t)S.sell_ptr.back(),
+                    (size_t)S.dtail, (size_t)tail_ld(S)};
+}
+
 size_t system_private_bytes(const StaticPattern& S, size_t vs, int m) {
-    const size_t n = S.n;
-    const size_t st = S.sell_ptr.back();
-    // The merged and row-major values and the sweep-order diagonal get 64
-    // bytes of slack: the kernels copy them in aligned 16-byte pieces.
-    return al256(S.cap * vs + 64) + al256(S.lci.size() * vs + 64) + al256(S.uci.size() * vs + 64) + al256(n * vs) +
-           al256(n * vs + 64) + al256(st * 8) + al256(st * 4) + al256((2 * (size_t)m + 8) * n * 8) +
-           al256((size_t)S.dtail * tail_ld(S) * vs) + al256((size_t)S.dtail * tail_ld(S) * 8);
+    return sys_private_bytes(host_sizes(S), vs, m);
 }
 
 char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m) {
-    const size_t n = S.n;
-    const size_t st = S.sell_ptr.back();
-    D.tail = p; p += al256((size_t)S.dtail * tail_ld(S) * vs);
-    D.tailw = S.dtail > 0 ? (double*)p : nullptr;
-    p += al256((size_t)S.dtail * tail_ld(S) * 8);
-    D.lu = p; p += al256(S.cap * vs + 64);
-    D.lval = p; p += al256(S.lci.size() * vs + 64);
-    D.uval = p; p += al256(S.uci.size() * vs + 64);
-    D.udiag = p; p += al256(n * vs);
-    D.udiag_bwd = p; p += al256(n * vs + 64);
-    D.sell64 = (double*)p; p += al256(st * 8);
-    D.sell32 = (float*)p; p += al256(st * 4);
-    D.work = (double*)p; p += al256((2 * (size_t)m + 8) * n * 8);
-    return p;
+    return sys_carve(D, p, host_sizes(S), vs, m);
 }
 
 size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& rplan) {
@@ -598,6 +686,12 @@ int check_opts(const lusp_batch_opts* o) {
         set_error("refactor_cluster must be 0 (auto) or 1..8");
         return LUSP_EARG;
     }
+    if (o->ladder < 0 || o->ladder > 3) { set_error("ladder must be 0..3"); return LUSP_EARG; }
+    if (o->ladder_slots < 0) { set_error("ladder_slots must be >= 0"); return LUSP_EARG; }
+    if (!(o->factor_shift >= 0.0) || !(o->hard_shift >= 0.0)) {
+        set_error("factor_shift and hard_shift must be >= 0");
+        return LUSP_EARG;
+    }
     if (o->refactor_threads != 0 &&
         (o->refactor_threads < 64 || o->refactor_threads > 1024 || o->refactor_threads % 32)) {
         set_error("refactor_threads must be 0 (auto) or 64..1024, a multiple of 32");
@@ -615,6 +709,7 @@ void fill_params(SolveParams& prm, const lusp_batch_opts& o) {
     prm.pivot_tol = o.pivot_tol;
     prm.refactor_mode = o.refactor_mode;
     prm.xtol = o.xtol > 0 ? o.xtol : 1e-8;
+    prm.shift = o.factor_shift;
 }
 
 int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, int nsys, LaunchArgs& a) {
@@ -656,6 +751,83 @@ int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& 
         a.dgrid = std::min(ntail, docc * sm_count());
     }
     return LUSP_OK;
+}
+
+int ladder_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, int cap, LaunchArgs& a,
+                 LadderPlan& lp, size_t pool) {
+    a.rungs = 0;
+    lp = LadderPlan{};
+    const int rungs = o.ladder == 1 ? 1 : o.ladder == 2 ? 2 : o.ladder == 3 ? 3 : 0;
+    if (rungs == 0 || o.prec != LUSP_MIXED || cap <= 0) return LUSP_OK;
+    lusp_batch_opts x = o;
+    x.prec = LUSP_FP64;
+    x.inner_prec = 0;
+    x.block_threads = 0;
+    x.ctas_per_sm = 0;
+    resolve_solve_shape(x, cap);
+    int rc = plan_for(pats, x, a.xplan);
+    if (rc != LUSP_OK) {
+        x.solve_sweep = 0;
+        rc = plan_for(pats, x, a.xplan);
+        if (rc != LUSP_OK) return rc;
+    }
+    int occ = 0;
+    rc = kernel_occupancy(LUSP_FP64, 0, a.xplan.bytes, x.block_threads, &occ);
+    if (rc != LUSP_OK) return rc;
+    if (occ < 1) { set_error("ladder solve kernel does not fit one SM (smem %zu)", a.xplan.bytes); return LUSP_EARG; }
+    a.xblock = x.block_threads;
+    a.xgrid = std::min(cap, occ * sm_count());
+    LaunchArgs r;
+    rc = refactor_setup(pats, x, cap, r);
+    if (rc != LUSP_OK) return rc;
+    a.xrplan = r.rplan;
+    a.xrblock = r.rblock;
+    a.xrgrid = r.rgrid;
+    a.xrcluster = r.rcluster;
+    a.xdplan = r.dplan;
+    a.xdblock = r.dblock;
+    a.xdgrid = r.dgrid;
+    fill_params(a.xprm, x);
+    a.xprm.shift = 0.0;
+    a.hard_shift = o.hard_shift > 0 ? o.hard_shift : 1e-7;
+    size_t stride = 0;
+    int colmax = 0;
+    for (auto* p : pats) {
+        stride = std::max(stride, system_private_bytes(p->S, 8, o.krylov));
+        colmax = std::max(colmax, p->S.max_col);
+    }
+    lp.pool = pool > 0 ? al256(pool) : (size_t)cap * stride;
+    lp.spill = spill_bytes(a.xrgrid, a.xrblock, colmax, a.xrplan);
+    lp.bytes = lp.pool + lp.spill + al256(sizeof(SysDev) * cap) + al256(sizeof(int) * cap);
+    a.rungs = rungs;
+    a.esc = EscDev{};
+    a.esc.cap = cap;
+    a.esc.m = o.krylov;
+    a.esc.pool = lp.pool;
+    a.esc.rtol = o.rtol;
+    a.esc.fail_bits = ST_SINGULAR | ST_PIVOT_WEAK | ST_STAGNATED | ST_NOT_CONVERGED | ST_NONFINITE |
+                      ST_WAIT_TIMEOUT | ST_CAPACITY;
+    return LUSP_OK;
+}
+
+void ladder_bind(LaunchArgs& a, const LadderPlan& lp, char* mem, int* queue) {
+    if (!a.rungs) return;
+    char* p = mem;
+    a.esc.base = p;
+    p += lp.pool;
+    a.esc.scratch = lp.spill ? (double*)p : nullptr;
+    p += lp.spill;
+    a.esc.slots = (SysDev*)p;
+    p += al256(sizeof(SysDev) * a.esc.cap);
+    a.esc.hard = (int*)p;
+    a.esc.ctl = queue + kLadderCtl;
+}
+
+// Ladder slots when the options leave them at 0: every system of a batch up
+// to 256, else an eighth of them (at least 256).
+static int ladder_cap(const lusp_batch_opts& o, int nsys) {
+    if (o.ladder_slots > 0) return std::min(o.ladder_slots, nsys);
+    return nsys <= 256 ? nsys : std::max(256, nsys / 8);
 }
 
 int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, SmemPlan& plan) {
@@ -713,6 +885,9 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     LaunchArgs& a = B->launch;
     rc = refactor_setup(B->pats, *o, nsys, a);
     if (rc != LUSP_OK) { delete B; return rc; }
+    LadderPlan lp;
+    rc = ladder_setup(B->pats, *o, ladder_cap(*o, nsys), a, lp);
+    if (rc != LUSP_OK) { delete B; return rc; }
     const size_t spill = spill_bytes(a.rgrid, a.rblock, colmax, a.rplan);
     const size_t total = base[nsys] + spill + al256(sizeof(SysStats) * nsys) + al256(sizeof(SysDev) * nsys) + 256;
     char* blk = nullptr;
@@ -743,6 +918,12 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     }
     e = cudaMemcpy(B->d_sys, B->h_sys.data(), sizeof(SysDev) * nsys, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { batch_free(B); return cuda_fail(e, "batch descriptor upload"); }
+    if (a.rungs) {
+        e = cudaMalloc(&B->d_ladder, lp.bytes);
+        if (e != cudaSuccess) { batch_free(B); return cuda_fail(e, "ladder device alloc"); }
+        B->bytes += lp.bytes;
+        ladder_bind(a, lp, B->d_ladder, B->d_queue);
+    }
     a.d_sys = B->d_sys;
     a.nsys = nsys;
     a.d_queue = B->d_queue;
@@ -764,6 +945,7 @@ void batch_free(BatchObj* B) {
         if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
     }
     if (B->d_block) cudaFree(B->d_block);
+    if (B->d_ladder) cudaFree(B->d_ladder);
     delete B;
 }
 

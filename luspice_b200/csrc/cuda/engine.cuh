@@ -48,6 +48,7 @@ struct PatternDev {
     // Dense trailing block: rows/columns [k0, n), dtail = n - k0 (0: none),
     // stored row-major with leading dimension tail_ld.
     int k0, dtail, tail_ld;
+    const int* a_diag;       // [n] slot offset of A(q_k, q_k) in column k, or -1
     const int* bwd_pos;      // [n] row -> index in bwd_order
     const int* fwd_ldesc;    // [nfwd_levels * 5] level descriptors (see host)
     const int* bwd_ldesc;    // [nbwd_levels * 5]
@@ -65,7 +66,8 @@ struct SysStats {
     int outer_iters;
     int status;
     int singular_col;
-    int pad_;
+    int rung;                // ladder rung of the result: 0 P-fast (the batch's
+                             // own precision), 1 P-safe, 2 P-hard
     // SM cycles (summed over warps): refactor waits for dependency columns,
     // gathers of their L parts, updates; refactor wall cycles of the CTA.
     long long cyc_wait, cyc_gather, cyc_update, cyc_refactor;
@@ -111,9 +113,73 @@ struct SolveParams {
     double pivot_tol;        // frozen-pivot acceptance threshold
     int refactor_mode;       // 0 staged gathers (cp.async), 1 per-dependency loads
     double xtol;             // forward-error target of the refinement
+    double shift;            // factor of A + shift * diag|A(i,i)| (0: A itself)
 };
 
 constexpr int kMaxKrylov = 64;
+
+// Sizes that fix one system's private device area.
+struct SysSizes {
+    size_t n, cap, nnz_l, nnz_u, sell, dtail, tail_ld;
+};
+
+__host__ __device__ inline SysSizes sizes_of(const PatternDev& P) {
+    return SysSizes{(size_t)P.n, (size_t)P.cap, (size_t)P.nnz_l, (size_t)P.nnz_u,
+                    (size_t)P.sell_total, (size_t)P.dtail, (size_t)P.tail_ld};
+}
+
+__host__ __device__ inline size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Private bytes of one system with factor values of vs bytes and Krylov
+// dimension m.  The merged and row-major values and the sweep-order
+// diagonal get 64 bytes of slack: the kernels copy them in aligned 16-byte
+// pieces.
+__host__ __device__ inline size_t sys_private_bytes(const SysSizes& z, size_t vs, int m) {
+    return al256(z.cap * vs + 64) + al256(z.nnz_l * vs + 64) + al256(z.nnz_u * vs + 64) + al256(z.n * vs) +
+           al256(z.n * vs + 64) + al256(z.sell * 8) + al256(z.sell * 4) + al256((2 * (size_t)m + 8) * z.n * 8) +
+           al256(z.dtail * z.tail_ld * vs) + al256(z.dtail * z.tail_ld * 8);
+}
+
+// Points the private arrays of D into p (sys_private_bytes of them); returns
+// the end.  The same layout on the host (batches, serving arenas) and on the
+// device (ladder slots).
+__host__ __device__ inline char* sys_carve(SysDev& D, char* p, const SysSizes& z, size_t vs, int m) {
+    D.tail = p; p += al256(z.dtail * z.tail_ld * vs);
+    D.tailw = z.dtail > 0 ? (double*)p : nullptr;
+    p += al256(z.dtail * z.tail_ld * 8);
+    D.lu = p; p += al256(z.cap * vs + 64);
+    D.lval = p; p += al256(z.nnz_l * vs + 64);
+    D.uval = p; p += al256(z.nnz_u * vs + 64);
+    D.udiag = p; p += al256(z.n * vs);
+    D.udiag_bwd = p; p += al256(z.n * vs + 64);
+    D.sell64 = (double*)p; p += al256(z.sell * 8);
+    D.sell32 = (float*)p; p += al256(z.sell * 4);
+    D.work = (double*)p; p += al256((2 * (size_t)m + 8) * z.n * 8);
+    return p;
+}
+
+// Device-side escalation ladder of one launch.  A system whose P-fast solve
+// (the batch's own fp32 factor and GMRES-IR) fails takes a slot: the solve
+// kernel that saw the failure points the slot's private arrays into fp64
+// storage taken from a pool, keeping the system's pattern, values,
+// right-hand side, solution and statistics, and the P-safe kernels (fp64 factor, GMRES-IR with the
+// fp64 factor as preconditioner) run over the taken slots.  A slot whose
+// P-safe solve fails again goes on to P-hard: the fp64 factor of
+// A + shift diag|A(i,i)| (the residual still uses A).
+struct EscDev {
+    int* ctl;                // [0] slots taken, [1] slots on the P-hard list,
+                             // [2..3] bytes of the storage pool taken (64 bit)
+    int* hard;               // [cap] slots escalated to P-hard
+    SysDev* slots;           // [cap] fp64 systems, filled by the device
+    char* base;              // storage pool: each slot takes its own system's
+    size_t pool;             // fp64 private bytes from it
+    double* scratch;         // refactor spill of the fp64 kernels (may be null)
+    int cap;                 // slots (0: no ladder)
+    int m;                   // Krylov dimension of the slots' workspace
+    int fail_bits;           // status bits that count as a failure (P-fast;
+                             // the fp64 rungs ignore a weak pivot alone)
+    double rtol;             // ... as does a final residual above rtol
+};
 
 // Shared-memory plan of one launch (same for every CTA).
 struct SmemPlan {

@@ -42,12 +42,40 @@ struct LaunchArgs {
     SmemPlan dplan{};                // dense trailing-block kernel (dgrid 0: none)
     int dblock = 512;
     int dgrid = 0;
+    // Escalation ladder after a mixed solve (rungs: bit 0 P-safe, bit 1
+    // P-hard; 0 none): fp64 kernels over the slots the solve kernel takes.
+    int rungs = 0;
+    EscDev esc{};
+    SmemPlan xplan{}, xrplan{}, xdplan{};
+    int xblock = 512, xgrid = 0, xrblock = 1024, xrgrid = 0, xrcluster = 1, xdblock = 512, xdgrid = 0;
+    SolveParams xprm{};              // P-safe parameters; P-hard adds the shift
+    double hard_shift = 1e-7;
 };
+
+// Queue words of one launch: three work counters per rung (P-fast, P-safe,
+// P-hard) in words 0..8, then the ladder's control words from word 10: two
+// slot counters and the 64-bit pool counter (words 12..13, 8-byte aligned
+// because the queue block is).
+constexpr int kQueueWords = 16;
+constexpr int kLadderCtl = 10;
+static_assert((kLadderCtl + 2) % 2 == 0 && kLadderCtl + 4 <= kQueueWords, "ladder control words");
 
 struct GraphEntry {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
+
+// Device memory and launch shapes of a ladder for up to cap systems of
+// pats (fp64 plans, storage pool, spill, slot descriptors, P-hard list).
+// pool: bytes of fp64 system storage (0: room for cap of the largest).
+struct LadderPlan {
+    size_t pool = 0, spill = 0, bytes = 0;
+};
+int ladder_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, int cap, LaunchArgs& a,
+                 LadderPlan& lp, size_t pool = 0);
+// Points the ladder into mem (lp.bytes, 256-byte aligned); queue: the
+// launch's queue words.
+void ladder_bind(LaunchArgs& a, const LadderPlan& lp, char* mem, int* queue);
 
 struct BatchObj {
     int nsys = 0;
@@ -59,6 +87,7 @@ struct BatchObj {
     SysStats* d_stats = nullptr;
     int* d_queue = nullptr;
     char* d_block = nullptr;
+    char* d_ladder = nullptr;        // escalation ladder storage (may be null)
     size_t bytes = 0;
     double* d_vals = nullptr;        // all systems' values, concatenated
     double* d_rhs = nullptr;         // all right-hand sides

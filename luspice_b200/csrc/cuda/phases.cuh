@@ -509,12 +509,16 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         for (int t = lane; t < len; t += 32) x[t] = 0.0;
         __syncwarp();
         const int a0 = P.a_ptr[k], a1 = P.a_ptr[k + 1];
+        // The factor of A + shift diag|A(i,i)|: the input's diagonal entry
+        // (duplicates summed first) gains shift times its magnitude.
+        const int adg = prm.shift != 0.0 ? P.a_diag[k] : -1;
         for (int t = a0 + lane; t < a1; t += 32) {
             const int dst = P.a_dst[t];
             if (t == a0 || P.a_dst[t - 1] != dst) {
                 double s = S.a_val[P.a_src[t]];
                 for (int u = t + 1; u < a1 && P.a_dst[u] == dst; u++)
                     s = __dadd_rn(s, S.a_val[P.a_src[u]]);
+                if (dst == adg) s = __dadd_rn(s, __dmul_rn(prm.shift, fabs(s)));
                 x[dst] = s;
             }
         }

@@ -289,6 +289,7 @@ bool ServerObj::try_launch(Flight& f) {
     // pick until everything (including the refactor spill area) fits.
     SmemPlan plan;
     LaunchArgs la;
+    LadderPlan lp;
     int grid = 0;
     size_t nval = 0, nvec = 0, spill = 0;
     const lusp_batch_opts o_req = o;
@@ -315,8 +316,24 @@ bool ServerObj::try_launch(Flight& f) {
         grid = std::min(nsp, occ * sm_count());
         if (refactor_setup(pats, o, nsp, la) != LUSP_OK) return false;
         spill = spill_bytes(la.rgrid, la.rblock, cm, la.rplan);
+        // Device-side escalation of the mixed path: a few ladder slots with
+        // room for the largest systems of the launch.
+        la.rungs = 0;
+        lp = LadderPlan{};
+        const int rungs = mode == MODE_FP64 ? 0 : opts.escalate == 1 ? 1 : opts.escalate == 2 ? 3 : 0;
+        if (rungs) {
+            lusp_batch_opts lo = o;
+            lo.ladder = rungs;
+            const int cap = std::min(nsp, std::max(2, (nsp + 15) / 16));
+            std::vector<size_t> sz;
+            for (Request* r : pick) sz.push_back(system_private_bytes(r->pe->pat->S, 8, o.krylov));
+            std::sort(sz.begin(), sz.end(), std::greater<size_t>());
+            size_t pool = 0;
+            for (int i = 0; i < cap; i++) pool += sz[i];
+            if (ladder_setup(pats, lo, cap, la, lp, pool) != LUSP_OK) return false;
+        }
         const size_t total = al(nval * 8) + 2 * al(nvec * 8) + privs + spill + al(sizeof(SysStats) * nsp) +
-                             al(sizeof(SysDev) * nsp) + 256;
+                             al(sizeof(SysDev) * nsp) + 256 + lp.bytes;
         if (total <= f.arena_bytes) break;
         if (nsp == 1) {
             Request* r = pick[0];
@@ -364,7 +381,10 @@ bool ServerObj::try_launch(Flight& f) {
     p += al(sizeof(SysDev) * ns);
     int* d_queue = (int*)p;
     p += 256;
+    char* d_ladder = p;
+    p += lp.bytes;
     if ((size_t)(p - a) > f.arena_bytes) return false;
+    ladder_bind(la, lp, d_ladder, d_queue);
     for (int i = 0; i < ns; i++) {
         hs[i].scratch = d_spill;
         hs[i].stats = d_stats + i;
@@ -435,7 +455,13 @@ void ServerObj::complete(Flight& f) {
         const SysStats& s = st[i];
         const bool failed = (s.status & fail) != 0 ||
                             (r->mode != MODE_FP64 && s.nres > 0 && !(s.res[s.nres - 1] <= opts.solver.rtol));
-        if (failed && r->mode != MODE_FP64 && opts.escalate) {
+        if (s.rung > 0) {
+            // Escalated on the device in the same launch: final.
+            r->escalated = true;
+            stats.escalated++;
+        } else if (failed && r->mode != MODE_FP64 && opts.escalate) {
+            // Not taken by a ladder (none, or no slot left): once more on
+            // the plain fp64 path.
             r->mode = MODE_FP64;
             r->escalated = true;
             queue.push_front(r);

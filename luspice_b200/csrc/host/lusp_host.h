@@ -51,6 +51,10 @@ struct StaticPattern {
     // give a_src (index into the input value array) and a_dst (slot offset
     // inside column k), sorted by a_dst (duplicates adjacent).
     std::vector<int> a_ptr, a_src, a_dst;
+    // a_diag[k]: slot offset inside column k of the input's diagonal entry
+    // A(q[k], q[k]), or -1 when the input has none (the factor shift of the
+    // escalation ladder adds to it).
+    std::vector<int> a_diag;
 
     // Row-major copies for the triangular solves, rows stored in level
     // order: strict-L row fwd_order[idx] is [lrp[idx], lrp[idx+1]) of lci

@@ -494,6 +494,7 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         for (int k = 0; k < n; k++) S.a_ptr[k + 1] += S.a_ptr[k];
         S.a_src.resize(S.nnz_a);
         S.a_dst.resize(S.nnz_a);
+        S.a_diag.assign(n, -1);
         std::vector<std::pair<int, int>> tmp;
         for (int k = 0; k < n; k++) {
             const int c = S.q[k];
@@ -504,6 +505,7 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
                 const int r = S.pinv[Ai[p]];
                 const int* it = std::lower_bound(rb, rb + len, r);
                 tmp.emplace_back((int)(it - rb), p);
+                if (Ai[p] == c) S.a_diag[k] = (int)(it - rb);
             }
             std::stable_sort(tmp.begin(), tmp.end(),
                              [](const std::pair<int, int>& a, const std::pair<int, int>& b) {

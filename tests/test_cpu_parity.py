@@ -226,6 +226,19 @@ def test_every_declared_symbol_is_exported(lib):
     assert "lu_factor_par_kernel" in syms and "trisolve_par_kernel" in syms
 
 
+def test_batch_opts_defaults_cover_every_field(lib):
+    """lusp_batch_opts_default sets every field the Python mirror declares
+    (the struct is mirrored field for field), the ladder off."""
+    from luspice_b200 import api
+    o = api.default_opts()
+    assert o.ladder == 0 and o.ladder_slots == 0
+    assert o.factor_shift == 0.0 and o.hard_shift == 1e-7
+    assert o.krylov == 30 and o.rtol == 1e-10 and o.xtol == 1e-8
+    s = _lib.ServerOpts()
+    lib.lusp_server_opts_default(C.byref(s))
+    assert s.escalate == 1 and s.solver.ladder == 0 and s.analysis_threads == 4
+
+
 def test_generators_deterministic_and_sized():
     a, b = mna.analog(989, 42), mna.analog(989, 42)
     assert np.array_equal(a.Ai, b.Ai) and np.array_equal(a.Ax, b.Ax)
