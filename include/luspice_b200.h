@@ -282,6 +282,33 @@ long long lusp_serve_submit(lusp_server *s, int n, const int *Ap, const int *Ai,
 int lusp_serve_poll(lusp_server *s, long long id, double *x, lusp_serve_result *res, int wait_ms);
 int lusp_server_get_stats(lusp_server *s, lusp_server_stats *st);
 
+/* ---- netlist matrix ingest (host; no device needed) ----
+ * COO triplets with 1-based indices, as s0 files and dsh_symbolic carry
+ * them.  cap: allocated entries. */
+typedef struct {
+    int n;
+    long long nnz, cap;
+    int *row, *col;
+    double *val;
+} lusp_coo;
+/* s0 file (header "n <n>", "A <i> <j> <val>" lines; spmv.h's format). */
+int lusp_read_s0_coo(const char *path, lusp_coo *A);
+/* Matrix Market coordinate file (real, integer or pattern; general,
+ * symmetric or skew-symmetric, the mirrored entries appended after each
+ * stored one), square. */
+int lusp_read_mtx_coo(const char *path, lusp_coo *A);
+/* Floating-node list: "F <row>" lines (1-based, other lines ignored) ->
+ * rows[0..*count) 0-based; LUSP_EALLOC with *count set when cap is short. */
+int lusp_read_flt(const char *path, int n, int *rows, int cap, int *count);
+/* pin > 0 onto the diagonal of each listed row (0-based): the first stored
+ * (i, i) entry gains pin, a row without one gets a new (i, i) = pin entry
+ * at the end (the replay programs' rule, bench/test_lu.c:71-93). */
+int lusp_coo_pin_rows(lusp_coo *A, const int *rows, int count, double pin);
+/* COO -> 0-based CSC (Ap[n+1], Ai/Ax[nnz]), entries of a column in
+ * storage order, duplicates kept. */
+int lusp_coo_to_csc(const lusp_coo *A, int *Ap, int *Ai, double *Ax);
+void lusp_coo_free(lusp_coo *A);
+
 /* ---- CSR SpMV with fp32 values (fp64 x, y and accumulation); the fp64
  * version is spmv_launch in spmv.h.  Device pointers. ---- */
 int lusp_csr_spmv32(int n, const int *d_rowptr, const int *d_colidx, const float *d_values,

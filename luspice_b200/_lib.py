@@ -66,6 +66,12 @@ class ServerStats(C.Structure):
                 ("max_batch_seen", C.c_longlong), ("pattern_gb", C.c_double)]
 
 
+class Coo(C.Structure):
+    """lusp_coo (luspice_b200.h): 1-based COO triplets."""
+    _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("cap", C.c_longlong),
+                ("row", C.POINTER(C.c_int)), ("col", C.POINTER(C.c_int)), ("val", C.POINTER(C.c_double))]
+
+
 class DshLuStatic(C.Structure):
     """dsh_lu_static (lu_static.h), field for field."""
     _fields_ = [("n", C.c_int), ("cnnz", C.c_long), ("lnnz", C.c_long), ("unnz", C.c_long),
@@ -161,6 +167,13 @@ SIGNATURES = {
     # level.h
     "dsh_level_compute": (C.c_int, [C.c_int, c_int_p, c_int_p, c_int_p, c_int_p]),
     "dsh_level_hist": (C.c_int, [C.c_int, c_int_p, C.c_int, c_int_p]),
+    # netlist ingest (luspice_b200.h)
+    "lusp_read_s0_coo": (C.c_int, [C.c_char_p, C.POINTER(Coo)]),
+    "lusp_read_mtx_coo": (C.c_int, [C.c_char_p, C.POINTER(Coo)]),
+    "lusp_read_flt": (C.c_int, [C.c_char_p, C.c_int, c_int_p, C.c_int, c_int_p]),
+    "lusp_coo_pin_rows": (C.c_int, [C.POINTER(Coo), c_int_p, C.c_int, C.c_double]),
+    "lusp_coo_to_csc": (C.c_int, [C.POINTER(Coo), c_int_p, c_int_p, c_double_p]),
+    "lusp_coo_free": (None, [C.POINTER(Coo)]),
     # spmv.h
     "read_s0_to_csr": (C.c_int, [C.c_char_p, C.POINTER(CSRMatrix)]),
     "csr_free": (None, [C.POINTER(CSRMatrix)]),

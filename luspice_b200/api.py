@@ -354,3 +354,35 @@ def sell_tune(n, rowptr, colidx, vals, kind: str = "fp32") -> dict:
     _check(L.load().lusp_sell_tune(int(n), L.ptr(rp, C.c_int), L.ptr(ci, C.c_int), L.ptr(v, C.c_double),
                                    Sell.KINDS[kind], C.byref(c), C.byref(sg), C.byref(us)), "lusp_sell_tune")
     return {"C": c.value, "sigma": sg.value, "us": us.value}
+
+
+def read_netlist(path, flt=None, pin: float = 0.0):
+    """Matrix of a netlist file (s0: "n <n>" + "A i j v" lines; Matrix
+    Market: a "%%MatrixMarket" banner) as 0-based CSC (n, Ap, Ai, Ax), with
+    the floating-node list of an .flt file pinned onto the diagonal when
+    pin > 0 (lusp_read_flt / lusp_coo_pin_rows)."""
+    lib = L.load()
+    path = str(path)
+    with open(path, "rb") as fh:
+        mtx = fh.read(14) == b"%%MatrixMarket"
+    A = L.Coo()
+    _check((lib.lusp_read_mtx_coo if mtx else lib.lusp_read_s0_coo)(path.encode(), C.byref(A)), "read " + path)
+    try:
+        if flt is not None and pin > 0:
+            cnt = C.c_int(0)
+            rc = lib.lusp_read_flt(str(flt).encode(), A.n, None, 0, C.byref(cnt))
+            if rc not in (0, 2):          # LUSP_EALLOC: only counted
+                _check(rc, "read " + str(flt))
+            rows = np.empty(max(cnt.value, 1), np.int32)
+            _check(lib.lusp_read_flt(str(flt).encode(), A.n, L.ptr(rows, C.c_int), rows.size, C.byref(cnt)),
+                   "read " + str(flt))
+            _check(lib.lusp_coo_pin_rows(C.byref(A), L.ptr(rows, C.c_int), cnt.value, pin), "pin")
+        n = A.n
+        Ap = np.empty(n + 1, np.int32)
+        Ai = np.empty(max(A.nnz, 1), np.int32)
+        Ax = np.empty(max(A.nnz, 1))
+        _check(lib.lusp_coo_to_csc(C.byref(A), L.ptr(Ap, C.c_int), L.ptr(Ai, C.c_int), L.ptr(Ax, C.c_double)),
+               "coo_to_csc")
+        return n, Ap, Ai[:A.nnz], Ax[:A.nnz]
+    finally:
+        lib.lusp_coo_free(C.byref(A))

@@ -28,7 +28,7 @@ LIB = LIBDIR / "libluspice_b200.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-C_SOURCES = ["host/selector.c", "host/level.c", "host/s0io.c"]
+C_SOURCES = ["host/selector.c", "host/level.c", "host/s0io.c", "host/ingest.c"]
 CXX_SOURCES = ["host/symbolic.cpp", "host/colamd.cpp", "host/lu_static.cpp"]
 CU_SOURCES = ["cuda/engine.cu", "cuda/capi.cu", "cuda/lu_gpu_par.cu", "cuda/spmv.cu", "cuda/noalloc.cu", "cuda/server.cu", "cuda/tune.cu"]
 HEADERS = sorted(str(p) for p in list(CSRC.rglob("*.h")) + list(CSRC.rglob("*.cuh")) + list(INCLUDE.glob("*.h")))
