@@ -126,8 +126,8 @@ typedef struct {
                                       from the last two corrections is <= xtol
                                       (default 1e-8) */
     int refactor_threads;          /* CTA size of the refactorization kernel: 0 auto
-                                      (1024 when the batch has at most one system per
-                                      SM, else 256), or 64..1024, a multiple of 32 */
+                                      (768 when the batch has at most one system per
+                                      SM, else 512), or 64..1024, a multiple of 32 */
     int refactor_cluster;          /* CTAs (one thread-block cluster) that share one
                                       system's refactorization: 0 auto (2 when every
                                       system of the batch gets its own pair of SMs,

@@ -951,7 +951,7 @@ __device__ __forceinline__ void sweep_barrier(int nthreads) {
 }
 
 template <typename VT, bool UPPER>
-__device__ void staged_sweep(int nlev, const int4* ld4, const int* lgl, const int* order, const int* rp,
+__device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* lgl, const int* order, const int* rp,
                              const int* ci, const VT* val, const VT* dgo, double* y,
                              char* stage, int cap_e, int cap_r) {
     const int NT = min((int)blockDim.x, kSweepThreads);
