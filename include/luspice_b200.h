@@ -104,7 +104,9 @@ typedef struct {
     int krylov;                    /* GMRES restart length (default 30, max 64) */
     int max_outer;                 /* outer corrections (default 3) */
     double rtol;                   /* ||b-Ax||/||b|| target (default 1e-10) */
-    double inner_rel;              /* inner stop vs current residual (default 1e-8) */
+    double inner_rel;              /* inner stop vs current residual (default 1e-4: the
+                                      outer loop corrects the rest; a tighter inner
+                                      stop only adds preconditioner applications) */
     double stag_ratio;             /* required residual reduction per outer (default 0.5) */
     double pivot_tol;              /* frozen-pivot acceptance (default 1e-3) */
     int block_threads;             /* CTA size of the solve kernel: 0 auto (512 when the
@@ -232,8 +234,9 @@ int lusp_batch_launch_count(const lusp_batch *b);
  * hash of (n, Ap, Ai), within hbm_budget_gb together with the launch arenas.
  * A system whose mixed-precision solve fails (IR stagnation, no
  * convergence, non-finite, weak or zero pivot) is escalated to fp64 as
- * `escalate` says: on the device in the same launch, or re-queued once on
- * the plain fp64 GPU path (LUSP_ST_ESCALATED in its result either way).  Results do not
+ * `escalate` says: on the device in the same launch, or re-queued once
+ * with an fp64 factor and GMRES-IR (LUSP_ST_ESCALATED in its result either
+ * way).  Results do not
  * depend on what else is in the launch (one CTA runs each system the same
  * way). */
 typedef struct {
@@ -246,9 +249,9 @@ typedef struct {
     int escalate;                  /* failed mixed systems: 0 kept as they are; 1 (default)
                                       the device ladder's P-safe rung in the same launch
                                       (lusp_batch_opts.ladder), and a system the ladder
-                                      had no slot for re-queued once on the plain fp64
-                                      path; 2 as 1 with P-safe then P-hard; 3 only the
-                                      re-queue on the plain fp64 path */
+                                      had no slot for re-queued once with an fp64 factor
+                                      and GMRES-IR; 2 as 1 with P-safe then P-hard; 3
+                                      only the re-queue */
     int analysis_threads;          /* host threads analysing new patterns (default 4) */
 } lusp_server_opts;
 

@@ -151,7 +151,7 @@ void lusp_batch_opts_default(lusp_batch_opts* o) {
     o->krylov = 30;
     o->max_outer = 3;
     o->rtol = 1e-10;
-    o->inner_rel = 1e-8;
+    o->inner_rel = 1e-4;
     o->stag_ratio = 0.5;
     o->pivot_tol = 1e-3;
     o->block_threads = 0;

@@ -627,8 +627,8 @@ template <typename VT, typename AT>
 static int launch_typed(const LaunchArgs& a, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(a.d_queue, 0, kQueueWords * sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "queue reset");
-    const int direct = (a.prec == LUSP_FP64 || (a.what & LUSP_RUN_DIRECT)) ? 1 : 0;
-    const bool ladder = a.rungs != 0 && !direct && (a.what & LUSP_RUN_SOLVE);
+    const int direct = ((a.prec == LUSP_FP64 && !a.ir64) || (a.what & LUSP_RUN_DIRECT)) ? 1 : 0;
+    const bool ladder = a.rungs != 0 && a.prec != LUSP_FP64 && !direct && (a.what & LUSP_RUN_SOLVE);
     EscDev none{};
     int rc = launch_rung<VT, AT>(a.d_sys, a.nsys, a.d_queue, nullptr, nullptr, a.what, main_shape(a), a.prm, direct,
                                  ladder ? a.esc : none, 0, st);

@@ -33,6 +33,7 @@ struct LaunchArgs {
     int prec = LUSP_MIXED;
     int inner = 0;
     int what = LUSP_RUN_BOTH;
+    int ir64 = 0;                    // fp64 factors solved by GMRES-IR, not directly
     int block = 256;
     int grid = 1;
     SmemPlan rplan{};                // refactorization kernel

@@ -49,9 +49,15 @@ struct PatternEntry {
     int fail_rc = LUSP_OK;
     int users = 0;                 // requests referencing it
     long long last_use = 0;
+    bool own = false;              // pivots chosen for one request's values:
+                                   // never matched by a lookup
 };
 
-enum Mode { MODE_MIXED = 0, MODE_MIXED_INNER64 = 1, MODE_FP64 = 2 };
+// MODE_FP64: the plain fp64 path (direct solve), for a server created in
+// fp64; MODE_FP64_IR: a failed mixed system once more with an fp64 factor
+// and GMRES-IR (the ladder's P-safe rung, run as its own launch).
+enum Mode { MODE_MIXED = 0, MODE_MIXED_INNER64 = 1, MODE_FP64 = 2, MODE_FP64_IR = 3 };
+static bool fp64_mode(int m) { return m == MODE_FP64 || m == MODE_FP64_IR; }
 
 struct Request {
     long long id = 0;
@@ -61,6 +67,7 @@ struct Request {
     int mode = MODE_MIXED;
     bool cache_hit = false;
     bool escalated = false;
+    bool repivoted = false;        // analysed again with its own values
     bool done = false;
     Clock::time_point t_submit, t_launch, t_done;
     lusp_serve_result res{};
@@ -108,6 +115,7 @@ struct ServerObj {
     bool try_launch(Flight& f);
     void complete(Flight& f);
     void evict_if_needed();
+    void release(PatternEntry* pe);
 };
 
 int ServerObj::init() {
@@ -196,6 +204,24 @@ void ServerObj::analysis_loop() {
     }
 }
 
+// A request is done with pe: one analysed for that request's own values
+// leaves the device at once.  Called with mu held.
+void ServerObj::release(PatternEntry* pe) {
+    pe->users--;
+    if (!pe->own || pe->users > 0 || pe->state == PAT_PENDING) return;
+    auto range = patterns.equal_range(pe->key);
+    for (auto it = range.first; it != range.second; ++it) {
+        if (it->second.get() != pe) continue;
+        if (pe->pat) {
+            pattern_bytes -= pe->pat->bytes;
+            pattern_free(pe->pat);
+            stats.patterns_resident--;
+        }
+        patterns.erase(it);
+        return;
+    }
+}
+
 // Least recently used patterns with no request referencing them leave the
 // device while the cache exceeds its share of the HBM budget.
 void ServerObj::evict_if_needed() {
@@ -231,7 +257,7 @@ bool ServerObj::try_launch(Flight& f) {
             r->t_done = Clock::now();
             r->res.latency_ms = ms_since(r->t_submit, r->t_done);
             r->done = true;
-            r->pe->users--;
+            release(r->pe);
             stats.completed++;
             it = queue.erase(it);
             cv_done.notify_all();
@@ -244,7 +270,7 @@ bool ServerObj::try_launch(Flight& f) {
         if (r->pe->state == PAT_READY) { mode = r->mode; break; }
     if (mode < 0) return false;
     lusp_batch_opts o = opts.solver;
-    o.prec = mode == MODE_FP64 ? LUSP_FP64 : LUSP_MIXED;
+    o.prec = fp64_mode(mode) ? LUSP_FP64 : LUSP_MIXED;
     o.inner_prec = mode == MODE_MIXED_INNER64 ? 1 : 0;
     const size_t vs = o.prec == LUSP_FP64 ? 8 : 4;
     // Choose requests (FIFO among ready ones of this mode) that fit.
@@ -271,7 +297,7 @@ bool ServerObj::try_launch(Flight& f) {
             r->t_done = Clock::now();
             r->res.latency_ms = ms_since(r->t_submit, r->t_done);
             r->done = true;
-            r->pe->users--;
+            release(r->pe);
             stats.completed++;
             queue.erase(std::find(queue.begin(), queue.end(), r));
             cv_done.notify_all();
@@ -320,11 +346,11 @@ bool ServerObj::try_launch(Flight& f) {
         // room for the largest systems of the launch.
         la.rungs = 0;
         lp = LadderPlan{};
-        const int rungs = mode == MODE_FP64 ? 0 : opts.escalate == 1 ? 1 : opts.escalate == 2 ? 3 : 0;
+        const int rungs = fp64_mode(mode) ? 0 : opts.escalate == 1 ? 1 : opts.escalate == 2 ? 3 : 0;
         if (rungs) {
             lusp_batch_opts lo = o;
             lo.ladder = rungs;
-            const int cap = std::min(nsp, std::max(2, (nsp + 15) / 16));
+            const int cap = std::min(nsp, std::max(4, (nsp + 7) / 8));
             std::vector<size_t> sz;
             for (Request* r : pick) sz.push_back(system_private_bytes(r->pe->pat->S, 8, o.krylov));
             std::sort(sz.begin(), sz.end(), std::greater<size_t>());
@@ -342,7 +368,7 @@ bool ServerObj::try_launch(Flight& f) {
             r->t_done = Clock::now();
             r->res.latency_ms = ms_since(r->t_submit, r->t_done);
             r->done = true;
-            r->pe->users--;
+            release(r->pe);
             stats.completed++;
             queue.erase(std::find(queue.begin(), queue.end(), r));
             cv_done.notify_all();
@@ -416,6 +442,7 @@ bool ServerObj::try_launch(Flight& f) {
     fill_params(la.prm, o);
     la.prec = o.prec;
     la.inner = o.inner_prec;
+    la.ir64 = mode == MODE_FP64_IR ? 1 : 0;
     la.what = LUSP_RUN_BOTH;
     la.block = o.block_threads;
     la.grid = grid;
@@ -454,15 +481,45 @@ void ServerObj::complete(Flight& f) {
         Request* r = f.reqs[i];
         const SysStats& s = st[i];
         const bool failed = (s.status & fail) != 0 ||
-                            (r->mode != MODE_FP64 && s.nres > 0 && !(s.res[s.nres - 1] <= opts.solver.rtol));
+                            (!fp64_mode(r->mode) && s.nres > 0 && !(s.res[s.nres - 1] <= opts.solver.rtol));
+        // The last step of the ladder: an fp64 solve that still fails with
+        // the frozen pivots (chosen for the pattern's first values) is
+        // analysed again with this request's own values (fresh partial
+        // pivoting) and solved once more with an fp64 factor and GMRES-IR.
+        const int hard = LUSP_ST_SINGULAR | LUSP_ST_STAGNATED | LUSP_ST_NOT_CONVERGED | LUSP_ST_NONFINITE;
+        const bool fp64_failed = (s.rung > 0 || r->mode == MODE_FP64_IR) &&
+                                 ((s.status & hard) != 0 || !(s.nres > 0 && s.res[s.nres - 1] <= opts.solver.rtol));
+        if (fp64_failed && !r->repivoted && opts.escalate) {
+            auto npe = std::make_unique<PatternEntry>();
+            npe->key = r->pe->key;
+            npe->n = r->n;
+            npe->Ap = r->pe->Ap;
+            npe->Ai = r->pe->Ai;
+            npe->Ax = r->vals;
+            npe->own = true;
+            npe->users = 1;
+            npe->last_use = ++clock;
+            PatternEntry* pe2 = npe.get();
+            patterns.emplace(npe->key, std::move(npe));
+            analysis_q.push_back(pe2);
+            cv_analysis.notify_one();
+            release(r->pe);
+            r->pe = pe2;
+            r->mode = MODE_FP64_IR;
+            r->repivoted = true;
+            if (!r->escalated) stats.escalated++;
+            r->escalated = true;
+            queue.push_front(r);
+            continue;
+        }
         if (s.rung > 0) {
             // Escalated on the device in the same launch: final.
             r->escalated = true;
             stats.escalated++;
-        } else if (failed && r->mode != MODE_FP64 && opts.escalate) {
-            // Not taken by a ladder (none, or no slot left): once more on
-            // the plain fp64 path.
-            r->mode = MODE_FP64;
+        } else if (failed && !fp64_mode(r->mode) && opts.escalate) {
+            // Not taken by a ladder (none, or no slot left): once more with
+            // an fp64 factor and GMRES-IR in a launch of its own.
+            r->mode = MODE_FP64_IR;
             r->escalated = true;
             queue.push_front(r);
             stats.escalated++;
@@ -481,8 +538,9 @@ void ServerObj::complete(Flight& f) {
         r->res.cache_hit = r->cache_hit ? 1 : 0;
         r->res.escalated = r->escalated ? 1 : 0;
         r->res.pattern_hash = r->pe->key;
-        r->pe->users--;
         r->pe->last_use = ++clock;
+        release(r->pe);
+        r->pe = nullptr;
         r->done = true;
         stats.completed++;
     }
@@ -592,7 +650,7 @@ long long lusp_serve_submit(lusp_server* s, int n, const int* Ap, const int* Ai,
         auto range = S->patterns.equal_range(key);
         for (auto it = range.first; it != range.second; ++it) {
             lusp::PatternEntry* c = it->second.get();
-            if (c->n == n && (int)c->Ai.size() == nnz && std::equal(c->Ap.begin(), c->Ap.end(), Ap) &&
+            if (!c->own && c->n == n && (int)c->Ai.size() == nnz && std::equal(c->Ap.begin(), c->Ap.end(), Ap) &&
                 std::equal(c->Ai.begin(), c->Ai.end(), Ai)) {
                 pe = c;
                 break;

@@ -93,3 +93,36 @@ def test_singular_pattern_reported(gpu):
     _, r = S.poll(rid, 120000)
     assert r["rc"] == 1
     S.close()
+
+
+def test_repivot_when_frozen_pivot_vanishes(gpu):
+    """A Newton step whose value at a frozen pivot is zero (a column with no
+    updates above its diagonal, so U(k,k) is that value): the mixed and fp64
+    frozen-pivot factors are singular, so the server analyses the request
+    again with its own values (fresh partial pivoting) and returns the fp64
+    oracle's answer."""
+    m = mna.analog(989, 42)
+    q = api.colamd(m.n, m.Ap, m.Ai)
+    f = api.pivot_factor(m.n, m.Ap, m.Ai, m.Ax, q)
+    rowat = np.empty(m.n, np.int64)
+    rowat[f["pinv"]] = np.arange(m.n)
+    bad = None
+    for k in range(m.n):
+        c = q[k]
+        if m.Ap[c + 1] - m.Ap[c] < 2 or f["Up"][k + 1] - f["Up"][k] != 1:
+            continue
+        col = np.arange(m.Ap[c], m.Ap[c + 1])
+        bad = m.Ax.copy()
+        bad[col[m.Ai[col] == rowat[k]][0]] = 0.0
+        if api.pivot_factor(m.n, m.Ap, m.Ai, bad, q)["singular_col"] < 0:
+            break
+    assert bad is not None
+    ref = oracle_solution(m, bad)
+    S = api.Server(max_batch=8, streams=1, arena_gb=0.5, staging_mb=32)
+    S.poll(S.submit(m.n, m.Ap, m.Ai, m.Ax, m.b), 120000)
+    x, r = S.poll(S.submit(m.n, m.Ap, m.Ai, bad, m.b), 120000)
+    assert r["rc"] == 0 and r["escalated"], r
+    assert rel_err(x, ref) <= TOL_REL, (rel_err(x, ref), r)
+    st = S.stats()
+    assert st["patterns_resident"] == 1     # the request's own analysis is gone
+    S.close()
