@@ -53,7 +53,9 @@ enum {
     LUSP_ST_ESCALATED = 128,  /* result comes from the fp64 path (server
                                  re-queue, or a ladder rung) */
     LUSP_ST_SHIFTED = 256,    /* ... from the ladder's P-hard rung */
-    LUSP_ST_LADDER_FULL = 512 /* the ladder had no slot left: P-fast result */
+    LUSP_ST_LADDER_FULL = 512,/* the ladder had no slot left: P-fast result */
+    LUSP_ST_FP16_OFF = 1024   /* inner_prec 2 asked for, the scaled range does
+                                 not fit fp16: fp32 inner products used */
 };
 
 enum { LUSP_MIXED = 0, LUSP_FP64 = 1 };
@@ -122,7 +124,11 @@ typedef struct {
                                       dependency with a search of the column's rows */
     int inner_prec;                /* A in the inner GMRES products (mixed path):
                                       0 fp32 values (default), 1 fp64 values (first
-                                      escalation step for ill-conditioned systems) */
+                                      escalation step for ill-conditioned systems),
+                                      2 Ruiz-scaled fp16 values where every scaled
+                                      nonzero lies in the fp16 normal range, checked
+                                      per system on the device at each solve (else
+                                      fp32, with LUSP_ST_FP16_OFF) */
     double xtol;                   /* forward-error target: the refinement stops when
                                       the residual is <= rtol and the error estimated
                                       from the last two corrections is <= xtol

@@ -18,7 +18,8 @@ RUN_REFACTOR, RUN_SOLVE, RUN_BOTH, RUN_DIRECT = 1, 2, 3, 4
 
 ST_SINGULAR, ST_PIVOT_WEAK, ST_STAGNATED, ST_NOT_CONVERGED = 1, 2, 4, 8
 ST_NONFINITE, ST_WAIT_TIMEOUT, ST_CAPACITY, ST_ESCALATED = 16, 32, 64, 128
-ST_SHIFTED, ST_LADDER_FULL = 256, 512
+ST_SHIFTED, ST_LADDER_FULL, ST_FP16_OFF = 256, 512, 1024
+INNER_FP32, INNER_FP64, INNER_FP16 = 0, 1, 2
 # Device-side escalation ladder (Batch(..., ladder=...)): rungs after a failed
 # mixed solve, inside the same launch.
 LADDER_OFF, LADDER_SAFE, LADDER_HARD, LADDER_SAFE_HARD = 0, 1, 2, 3

@@ -2,6 +2,7 @@
 // combination order (results are run-to-run deterministic), bounded waits
 // on shared-memory ready bits, and status codes.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -20,6 +21,8 @@ enum : int {
     ST_ESCALATED = 128,    // the result comes from an fp64 rung of the ladder
     ST_SHIFTED = 256,      // ... from the P-hard rung (factor of A + shift diag|A|)
     ST_LADDER_FULL = 512,  // the ladder had no free slot: P-fast result kept
+    ST_FP16_OFF = 1024,    // fp16 inner products asked for, but the Ruiz-scaled
+                           // values leave the fp16 normal range: fp32 used
 };
 
 // Spin bound for waits on shared-memory ready bits inside one CTA: about a
@@ -87,6 +90,27 @@ __device__ __forceinline__ double block_sum(double v, double* scratch) {
     }
     __syncthreads();
     return scratch[32];
+}
+
+// Block-wide maximum / minimum (all threads call, all receive the result).
+__device__ __forceinline__ double block_max(double v, double* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    v = warp_max(v);
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        double s = lane < nw ? scratch[lane] : -INFINITY;
+        s = warp_max(s);
+        if (lane == 0) scratch[32] = s;
+    }
+    __syncthreads();
+    return scratch[32];
+}
+
+__device__ __forceinline__ double block_min(double v, double* scratch) {
+    return -block_max(-v, scratch);
 }
 
 template <typename T> struct ValTraits;

@@ -556,6 +556,7 @@ int refactor_occupancy(int prec, size_t smem, int block, int* occ) {
 int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ) {
     if (prec == LUSP_FP64) return kernel_prepare<double, double>(smem, block, occ);
     if (inner == 1) return kernel_prepare<float, double>(smem, block, occ);
+    if (inner == 2) return kernel_prepare<float, __half>(smem, block, occ);
     return kernel_prepare<float, float>(smem, block, occ);
 }
 
@@ -657,6 +658,7 @@ static int launch_typed(const LaunchArgs& a, cudaStream_t st) {
 int launch_systems(const LaunchArgs& a, cudaStream_t st) {
     if (a.prec == LUSP_FP64) return launch_typed<double, double>(a, st);
     if (a.inner == 1) return launch_typed<float, double>(a, st);
+    if (a.inner == 2) return launch_typed<float, __half>(a, st);
     return launch_typed<float, float>(a, st);
 }
 
@@ -703,7 +705,7 @@ int check_opts(const lusp_batch_opts* o) {
         return LUSP_EARG;
     }
     if (o->ctas_per_sm < 0) { set_error("ctas_per_sm must be >= 0"); return LUSP_EARG; }
-    if (o->inner_prec < 0 || o->inner_prec > 1) { set_error("bad inner_prec"); return LUSP_EARG; }
+    if (o->inner_prec < 0 || o->inner_prec > 2) { set_error("bad inner_prec"); return LUSP_EARG; }
     if (o->refactor_cluster < 0 || o->refactor_cluster > 8) {
         set_error("refactor_cluster must be 0 (auto) or 1..8");
         return LUSP_EARG;

@@ -91,6 +91,9 @@ struct SysDev {
     void* udiag_bwd;         // [n] U(k,k) (VT) in backward sweep order
     double* sell64;          // [sell_total] A in SELL, fp64
     float* sell32;           // [sell_total] A in SELL, fp32
+    void* sell16;            // [sell_total] Ruiz-scaled A in SELL, fp16 (__half)
+    double* rs;              // [n] Ruiz row scaling (position space)
+    double* cs;              // [n] Ruiz column scaling
     const double* b;         // [n] right-hand side, original row order
     double* x;               // [n] solution, original column order
     double* work;            // workspace (see solve phase)
@@ -137,7 +140,8 @@ __host__ __device__ inline size_t al256(size_t b) { return (b + 255) & ~(size_t)
 __host__ __device__ inline size_t sys_private_bytes(const SysSizes& z, size_t vs, int m) {
     return al256(z.cap * vs + 64) + al256(z.nnz_l * vs + 64) + al256(z.nnz_u * vs + 64) + al256(z.n * vs) +
            al256(z.n * vs + 64) + al256(z.sell * 8) + al256(z.sell * 4) + al256((2 * (size_t)m + 8) * z.n * 8) +
-           al256(z.dtail * z.tail_ld * vs) + al256(z.dtail * z.tail_ld * 8);
+           al256(z.dtail * z.tail_ld * vs) + al256(z.dtail * z.tail_ld * 8) + al256(z.sell * 2) +
+           2 * al256(z.n * 8);
 }
 
 // Points the private arrays of D into p (sys_private_bytes of them); returns
@@ -155,6 +159,9 @@ __host__ __device__ inline char* sys_carve(SysDev& D, char* p, const SysSizes& z
     D.sell64 = (double*)p; p += al256(z.sell * 8);
     D.sell32 = (float*)p; p += al256(z.sell * 4);
     D.work = (double*)p; p += al256((2 * (size_t)m + 8) * z.n * 8);
+    D.sell16 = p; p += al256(z.sell * 2);
+    D.rs = (double*)p; p += al256(z.n * 8);
+    D.cs = (double*)p; p += al256(z.n * 8);
     return p;
 }
 

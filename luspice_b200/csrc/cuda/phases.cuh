@@ -4,6 +4,8 @@
 #pragma once
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include "engine.cuh"
 
 namespace lusp {
@@ -26,7 +28,7 @@ struct Smem {
 };
 
 // Status bits that describe a solve (cleared when a new solve starts).
-constexpr int kSolveBits = ST_STAGNATED | ST_NOT_CONVERGED | ST_NONFINITE | ST_WAIT_TIMEOUT;
+constexpr int kSolveBits = ST_STAGNATED | ST_NOT_CONVERGED | ST_NONFINITE | ST_WAIT_TIMEOUT | ST_FP16_OFF;
 
 // Slot of row i among rows[lo, hi) (ascending), or -1.
 __device__ __forceinline__ int find_slot(const int* rows, int lo, int hi, int i) {
@@ -1159,6 +1161,126 @@ __device__ void cta_spmv(const PatternDev& P, const AT* vals, const double* xin,
     }
 }
 
+// ---------------------------------------------------------------------------
+// fp16 inner products.  Ruiz equilibration of A (position space, SELL
+// order) gives rs, cs with every row and column maximum of |rs_i a_ij cs_j|
+// near 1; the scaled values are stored in fp16 only when every nonzero one
+// lies in the fp16 normal range [2^-14, 65504], so no value underflows or
+// overflows in storage (else the fp32 values are used and ST_FP16_OFF says
+// so).  The scaling is the one lusp_sell_create applies (spmv.cu,
+// lusp_ruiz_csr), operation for operation: row maxima of |a| rs_i cs_j,
+// rs_i /= sqrt(max), then column maxima, cs_j /= sqrt(max), until every
+// maximum is within 1e-6 of 1, at most kRuizSweeps sweeps.  The reference
+// equilibrates the same way on the host (bench/test_lu_gpu_par.cu:237-260,
+// 30 sweeps, early stop 1e-6).
+// ---------------------------------------------------------------------------
+constexpr int kRuizSweeps = 30;
+
+// colmax: n doubles of global scratch.  Returns whether fp16 storage fits.
+__device__ bool ruiz_sell16(const SysDev& S, const PatternDev& P, double* colmax, Smem& sm) {
+    const int n = P.n;
+    double* rs = S.rs;
+    double* cs = S.cs;
+    __half* h = (__half*)S.sell16;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        rs[i] = 1.0;
+        cs[i] = 1.0;
+    }
+    __syncthreads();
+    const int nq = 32 * P.nslices;
+    for (int it = 0; it < kRuizSweeps; it++) {
+        double dev = 0.0;
+        // Rows: one thread per SELL row (a row's entries are one lane of its slice).
+        for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+            const int r = P.sell_perm[q];
+            if (r < 0) continue;
+            const int base = P.sell_ptr[q >> 5], L = (P.sell_ptr[(q >> 5) + 1] - base) >> 5;
+            const double rr = rs[r];
+            double m = 0.0;
+            for (int t = 0; t < L; t++) {
+                const int e = base + (t << 5) + (q & 31);
+                if (P.sell_src[e] >= 0) m = fmax(m, fabs(S.sell64[e]) * rr * cs[P.sell_col[e]]);
+            }
+            if (m > 0.0) {
+                rs[r] = rr / sqrt(m);
+                dev = fmax(dev, fabs(1.0 - m));
+            }
+        }
+        for (int j = threadIdx.x; j < n; j += blockDim.x) colmax[j] = 0.0;
+        __syncthreads();
+        // Columns: maxima by atomic max on the bit patterns (non-negative).
+        for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+            const int r = P.sell_perm[q];
+            if (r < 0) continue;
+            const int base = P.sell_ptr[q >> 5], L = (P.sell_ptr[(q >> 5) + 1] - base) >> 5;
+            const double rr = rs[r];
+            for (int t = 0; t < L; t++) {
+                const int e = base + (t << 5) + (q & 31);
+                if (P.sell_src[e] < 0) continue;
+                const int c = P.sell_col[e];
+                const double a = fabs(S.sell64[e]) * rr * cs[c];
+                atomicMax((unsigned long long*)(colmax + c), (unsigned long long)__double_as_longlong(a));
+            }
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double m = colmax[j];
+            if (m > 0.0) {
+                cs[j] = cs[j] / sqrt(m);
+                dev = fmax(dev, fabs(1.0 - m));
+            }
+        }
+        dev = block_max(dev, sm.red);
+        if (dev < 1e-6) break;
+    }
+    // fp16 values (padding 0) and the range of the scaled nonzeros.
+    double mn = INFINITY, mx = 0.0;
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        const int r = P.sell_perm[q];
+        const int base = P.sell_ptr[q >> 5], L = (P.sell_ptr[(q >> 5) + 1] - base) >> 5;
+        for (int t = 0; t < L; t++) {
+            const int e = base + (t << 5) + (q & 31);
+            double a = 0.0;
+            if (r >= 0 && P.sell_src[e] >= 0) a = S.sell64[e] * rs[r] * cs[P.sell_col[e]];
+            h[e] = __double2half(a);
+            const double aa = fabs(a);
+            if (aa != 0.0) {
+                mn = fmin(mn, aa);
+                mx = fmax(mx, aa);
+            }
+        }
+    }
+    mn = block_min(mn, sm.red);
+    mx = block_max(mx, sm.red);
+    return mn >= 6.103515625e-05 && mx <= 65504.0;
+}
+
+// out = A x with the fp16 values: out_r = (sum_c h_rc (x_c / cs_c)) / rs_r,
+// fp64 accumulation; xc: n doubles of scratch.
+__device__ void cta_spmv16(const PatternDev& P, const __half* vals, const double* rs, const double* cs,
+                           const double* xin, double* xc, double* out) {
+    for (int i = threadIdx.x; i < P.n; i += blockDim.x) xc[i] = xin[i] / cs[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int s = warp; s < P.nslices; s += nw) {
+        const int base = P.sell_ptr[s];
+        const int L = (P.sell_ptr[s + 1] - base) >> 5;
+        double acc = 0.0, a1 = 0.0;
+        int t = 0;
+        for (; t + 1 < L; t += 2) {
+            const int e = base + (t << 5) + lane;
+            acc = fma((double)__half2float(vals[e]), xc[P.sell_col[e]], acc);
+            a1 = fma((double)__half2float(vals[e + 32]), xc[P.sell_col[e + 32]], a1);
+        }
+        if (t < L) {
+            const int e = base + (t << 5) + lane;
+            acc = fma((double)__half2float(vals[e]), xc[P.sell_col[e]], acc);
+        }
+        const int row = P.sell_perm[(s << 5) + lane];
+        if (row >= 0) out[row] = (acc + a1) / rs[row];
+    }
+}
+
 __device__ __forceinline__ double cta_dot(const double* a, const double* b, int n, Smem& sm) {
     double s = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) s = fma(a[i], b[i], s);
@@ -1247,7 +1369,8 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
     const VT* uval = (const VT*)S.uval;
     const VT* udiag = (const VT*)S.udiag;
     const VT* tail = (const VT*)S.tail;
-    const AT* ainner = (const AT*)(sizeof(AT) == 8 ? (const void*)S.sell64 : (const void*)S.sell32);
+    constexpr bool kHalf = std::is_same<AT, __half>::value;
+    const void* ainner = sizeof(AT) == 8 ? (const void*)S.sell64 : (const void*)S.sell32;
     int bad = 0;
     int status = 0;
     int inner_total = 0, outer_done = 0, nres = 0;
@@ -1264,6 +1387,12 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         desc = d;
     }
     __syncthreads();
+    bool use16 = false;
+    if constexpr (kHalf) {
+        // V holds nothing yet: its first n doubles serve the column maxima.
+        use16 = ruiz_sell16(S, P, V, sm);
+        if (!use16 && threadIdx.x == 0) atomicOr(&S.stats->status, (int)ST_FP16_OFF);
+    }
     const double nb = sqrt(cta_dot(bt, bt, n, sm));
     if (!(nb > 0.0)) {
         for (int i = threadIdx.x; i < n; i += blockDim.x) S.x[i] = 0.0;
@@ -1326,7 +1455,13 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
             double* zj = Zb + (size_t)j * n;
             for (int e = threadIdx.x; e < n; e += blockDim.x) zj[e] = y[e];
             const long long tsp = clock64();
-            cta_spmv<AT, false>(P, ainner, y, nullptr, w);
+            if constexpr (kHalf) {
+                // r is free inside the inner loop: it holds x / cs.
+                if (use16) cta_spmv16(P, (const __half*)S.sell16, S.rs, S.cs, y, r, w);
+                else cta_spmv<float, false>(P, S.sell32, y, nullptr, w);
+            } else {
+                cta_spmv<AT, false>(P, (const AT*)ainner, y, nullptr, w);
+            }
             __syncthreads();
             if (threadIdx.x == 0) S.stats->cyc_spmv += clock64() - tsp;
             const double wn0 = sqrt(cta_dot(w, w, n, sm));

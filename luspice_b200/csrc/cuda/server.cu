@@ -271,7 +271,7 @@ bool ServerObj::try_launch(Flight& f) {
     if (mode < 0) return false;
     lusp_batch_opts o = opts.solver;
     o.prec = fp64_mode(mode) ? LUSP_FP64 : LUSP_MIXED;
-    o.inner_prec = mode == MODE_MIXED_INNER64 ? 1 : 0;
+    o.inner_prec = mode == MODE_MIXED_INNER64 ? 1 : (opts.solver.inner_prec == 2 ? 2 : 0);
     const size_t vs = o.prec == LUSP_FP64 ? 8 : 4;
     // Choose requests (FIFO among ready ones of this mode) that fit.
     std::vector<Request*> pick;
