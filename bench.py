@@ -3,7 +3,7 @@
 Workload (one step): the 63x64 power-grid MNA matrix plus 18 Vdd pad rows
 (n = 4050), 50 Newton refactorizations on the same pattern with element
 values perturbed log-normally (sigma = 0.1), each followed by a full solve:
-fp32 factors (frozen pivots) + fp64 GMRES-IR (restart 30, rtol 1e-10), all
+fp32 factors (frozen pivots) + fp64 GMRES-IR (restart 30, inner stop 1e-4, rtol 1e-10), all
 50 systems in one CUDA graph of three persistent kernels (sparse refactor,
 dense trailing block, solve).  `value` counts only systems whose
 solution is within rel-L2 1e-6 of the fp64 oracle (checked after timing).
@@ -42,7 +42,7 @@ NSYS = 50
 HOST_AHEAD_CYCLES = 200_000
 WORKLOAD = ("power-grid MNA n=4050 (63x64 mesh + 18 Vdd pads), 50 Newton refactors on one "
             "pattern (log-normal sigma=0.1 element perturbation), fp32 factor + fp64 GMRES-IR "
-            "(restart 30, rtol 1e-10), one graph of three persistent kernels per step")
+            "(restart 30, inner stop 1e-4, rtol 1e-10, forward-error stop 1e-8), one graph of three persistent kernels per step")
 
 
 def peaks():

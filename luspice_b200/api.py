@@ -344,7 +344,7 @@ def autotune(m, nsys: int, prec: int = MIXED, **opts) -> dict:
     d, ms = C.c_int(), C.c_double()
     _check(lib.lusp_tune(int(m.n), L.ptr(Ap, C.c_int), L.ptr(Ai, C.c_int), L.ptr(Ax, C.c_double),
                          L.ptr(b, C.c_double), int(nsys), C.byref(o), C.byref(d), C.byref(ms)), "lusp_tune")
-    keys = ("refactor_cluster", "block_threads", "ctas_per_sm", "solve_sweep")
+    keys = ("refactor_threads", "refactor_cluster", "block_threads", "ctas_per_sm", "solve_sweep")
     return {"dense_tail": d.value, "opts": {k: getattr(o, k) for k in keys}, "ms": ms.value}
 
 

@@ -81,10 +81,16 @@ int lusp_tune(int n, const int* Ap, const int* Ai, const double* Ax, const doubl
         lusp_pattern* P = nullptr;
         if (lusp_pattern_create_ex(n, Ap, Ai, Ax, nullptr, d, &P) != LUSP_OK) continue;
         std::vector<lusp_pattern*> pats(nsys, P);
+        // Refactor CTA: the automatic size and its neighbour (one CTA per SM
+        // when every system has an SM, else two per SM).
+        const bool few = nsys <= lusp::sm_count();
+        const int rts[2] = {few ? 768 : 512, few ? 1024 : 768};
+        for (int rt : rts)
         for (int rcl : {1, 2})
             for (int bt : {256, 512})
                 for (int sw : {0, 1}) {
                     lusp_batch_opts o = *opts;
+                    o.refactor_threads = rt;
                     o.refactor_cluster = rcl;
                     o.block_threads = bt;
                     o.ctas_per_sm = bt == 512 ? 1 : 2;
