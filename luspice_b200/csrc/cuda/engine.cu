@@ -459,9 +459,9 @@ void make_dense_plan(const std::vector<PatternObj*>& pats, int threads, SmemPlan
     const size_t budget = 227 * 1024;
     plan.bytes = fixed;
     if (dmax == 0) return;
-    // Panel [D][nb] + U tile [nb][128] + nb column maxima + 4 cycle
-    // counters: the widest panel (32, 16, 8) that fits.
-    auto dneed = [&](int nb) { return fixed + 8 * ((size_t)dmax * nb + (size_t)nb * 128 + nb + 4); };
+    // Panel [D][nb + 1] (padded rows) + U tile [nb][128] + nb column maxima
+    // + 4 cycle counters: the widest panel (32, 16, 8) that fits.
+    auto dneed = [&](int nb) { return fixed + 8 * ((size_t)dmax * (nb + 1) + (size_t)nb * 128 + nb + 4); };
     int nb = 32;
     while (nb > 8 && dneed(nb) > budget) nb /= 2;
     plan.tnb = nb;

@@ -145,9 +145,10 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
                                   const SolveParams& prm, double& minpiv, double& minratio, int& bad,
                                   SysStats* st) {
     const int D = P.dtail, ld = P.tail_ld, k0 = P.k0, nb = plan.tnb;
+    const int ps = nb + 1;   // panel row stride: odd, so a lane per row hits distinct banks
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
-    double* pan = (double*)sm.uni;                                           // [D][nb]
-    double* ut = pan + (size_t)D * nb;                                       // [nb][128]
+    double* pan = (double*)sm.uni;                                           // [D][ps]
+    double* ut = pan + (size_t)D * ps;                                       // [nb][128]
     unsigned long long* cmax = (unsigned long long*)(ut + (size_t)nb * 128); // [nb]
     long long* ctr = (long long*)(cmax + nb);   // [4] stage cycles (thread 0)
     if (tid == 0) {
@@ -158,49 +159,36 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
         const int w = min(nb, D - jb), R = D - jb;
         for (int t = tid; t < R * nb; t += nt) {
             const int r = t / nb, c = t - r * nb;
-            pan[t] = c < w ? W[(size_t)(jb + r) * ld + jb + c] : 0.0;
+            pan[r * ps + c] = c < w ? W[(size_t)(jb + r) * ld + jb + c] : 0.0;
         }
         if (tid < nb) cmax[tid] = 0ull;
         __syncthreads();
-        // Panel: unblocked elimination.  Per column: the multipliers (one
-        // thread per row, all divisions in flight together), then the update
-        // of the columns to the right (a warp per row, lanes = columns).
+        // Panel: unblocked elimination, a lane per row and a warp per 32
+        // rows, so a row's multiplier and its update stay inside one warp:
+        // one CTA barrier per column (the pivot row must be final for all).
         const int warp = tid >> 5, nw = nt >> 5;
         for (int c = 0; c < w; c++) {
-            const double piv = pan[c * nb + c];
+            const double piv = pan[c * ps + c];
+            const double* urow = pan + (size_t)c * ps;
             double lm = 0.0;
-            for (int r = c + 1 + tid; r < R; r += nt) {
-                const double v = pan[r * nb + c];
-                lm = fmax(lm, fabs(v));
-                pan[r * nb + c] = (double)ValTraits<VT>::to(__ddiv_rn(v, piv));
+            for (int r0 = c + 1 + warp * 32; r0 < R; r0 += nw * 32) {
+                const int r = r0 + lane;
+                if (r < R) {
+                    double* row = pan + (size_t)r * ps;
+                    const double v = row[c];
+                    lm = fmax(lm, fabs(v));
+                    const double l = (double)ValTraits<VT>::to(__ddiv_rn(v, piv));
+                    row[c] = l;
+                    for (int j = c + 1; j < w; j++) row[j] = __dsub_rn(row[j], __dmul_rn(l, urow[j]));
+                }
             }
             lm = warp_max(lm);
             if (lane == 0 && lm > 0.0) atomicMax(&cmax[c], (unsigned long long)__double_as_longlong(lm));
             __syncthreads();
-            if (c + 1 < w) {
-                const double uc = lane < w ? pan[c * nb + lane] : 0.0;
-                const bool act = lane > c && lane < w;
-                int r = c + 1 + warp;
-                for (; r + nw < R; r += 2 * nw) {
-                    double* r0 = pan + (size_t)r * nb;
-                    double* r1 = r0 + (size_t)nw * nb;
-                    const double l0 = r0[c], l1 = r1[c];
-                    if (act) {
-                        const double a0 = r0[lane], a1 = r1[lane];
-                        r0[lane] = __dsub_rn(a0, __dmul_rn(l0, uc));
-                        r1[lane] = __dsub_rn(a1, __dmul_rn(l1, uc));
-                    }
-                }
-                if (r < R && act) {
-                    double* r0 = pan + (size_t)r * nb;
-                    r0[lane] = __dsub_rn(r0[lane], __dmul_rn(r0[c], uc));
-                }
-                __syncthreads();
-            }
         }
         if (tid < w) {
             const int c = tid;
-            const double piv = pan[c * nb + c];
+            const double piv = pan[c * ps + c];
             const double ap = fabs(piv);
             const double amax = __longlong_as_double((long long)cmax[c]);
             if (!(ap > 0.0) || !isfinite(piv)) {
@@ -214,7 +202,7 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
         }
         for (int t = tid; t < R * nb; t += nt) {
             const int r = t / nb, c = t - r * nb;
-            if (c < w) W[(size_t)(jb + r) * ld + jb + c] = pan[t];
+            if (c < w) W[(size_t)(jb + r) * ld + jb + c] = pan[r * ps + c];
         }
         __syncthreads();
         if (tid == 0) {
@@ -241,13 +229,13 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
                     for (int c = 0; c < 8; c++)
 #pragma unroll
                         for (int r = 0; r < 8; r++)
-                            if (g + r < w) u[r] = __dsub_rn(u[r], __dmul_rn(pan[(g + r) * nb + g2 + c], v[c]));
+                            if (g + r < w) u[r] = __dsub_rn(u[r], __dmul_rn(pan[(g + r) * ps + g2 + c], v[c]));
                 }
 #pragma unroll
                 for (int c = 0; c < 8; c++)
 #pragma unroll
                     for (int r = c + 1; r < 8; r++)
-                        if (g + r < w) u[r] = __dsub_rn(u[r], __dmul_rn(pan[(g + r) * nb + g + c], u[c]));
+                        if (g + r < w) u[r] = __dsub_rn(u[r], __dmul_rn(pan[(g + r) * ps + g + c], u[c]));
 #pragma unroll
                 for (int r = 0; r < 8; r++)
                     if (g + r < w) W[(size_t)(jb + g + r) * ld + col] = u[r];
@@ -279,14 +267,14 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     const int row = rw + q * nw;
-                    lo[q] = row < D ? q * nw * nb : 0;   // rows past the block reuse rw's multipliers
+                    lo[q] = row < D ? q * nw * ps : 0;   // rows past the block reuse rw's multipliers
 #pragma unroll
                     for (int j = 0; j < 4; j++) {
                         const int col = q0 + lane + 32 * j;
                         acc[q][j] = (row < D && col < D) ? W[(size_t)row * ld + col] : 0.0;
                     }
                 }
-                const double* l0 = pan + (size_t)(rw - jb) * nb;
+                const double* l0 = pan + (size_t)(rw - jb) * ps;
                 for (int c = 0; c < w; c++) {
                     double u[4];
 #pragma unroll
