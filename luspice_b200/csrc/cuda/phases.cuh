@@ -179,7 +179,19 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
                     lm = fmax(lm, fabs(v));
                     const double l = (double)ValTraits<VT>::to(__ddiv_rn(v, piv));
                     row[c] = l;
-                    for (int j = c + 1; j < w; j++) row[j] = __dsub_rn(row[j], __dmul_rn(l, urow[j]));
+                    // Eight entries and their pivot-row values are loaded
+                    // before any is stored (the stores could alias the loads).
+                    for (int j0 = c + 1; j0 < w; j0 += 8) {
+                        double a[8], u[8];
+#pragma unroll
+                        for (int q = 0; q < 8; q++) {
+                            a[q] = j0 + q < w ? row[j0 + q] : 0.0;
+                            u[q] = j0 + q < w ? urow[j0 + q] : 0.0;
+                        }
+#pragma unroll
+                        for (int q = 0; q < 8; q++)
+                            if (j0 + q < w) row[j0 + q] = __dsub_rn(a[q], __dmul_rn(l, u[q]));
+                    }
                 }
             }
             lm = warp_max(lm);
