@@ -548,6 +548,24 @@ static int dense_prepare(size_t smem, int block, int* occ) {
     return prepare_kernel(dense_kernel<VT>, smem, block, occ, &granted, mu);
 }
 
+// Loads every kernel of the engine into the current context (CUDA loads a
+// module's functions lazily, at their first use; a long-lived caller such as
+// the serving loop pays that once at creation instead of inside a request).
+int preload_kernels() {
+    const void* fns[] = {
+        (const void*)refactor_fn<float>(512), (const void*)refactor_fn<float>(640), (const void*)refactor_fn<float>(768),
+        (const void*)refactor_fn<double>(512), (const void*)refactor_fn<double>(640),
+        (const void*)refactor_fn<double>(768), (const void*)dense_kernel<float>, (const void*)dense_kernel<double>,
+        (const void*)solve_kernel<float, float>, (const void*)solve_kernel<float, double>,
+        (const void*)solve_kernel<float, __half>, (const void*)solve_kernel<double, double>};
+    for (const void* f : fns) {
+        cudaFuncAttributes at;
+        cudaError_t e = cudaFuncGetAttributes(&at, f);
+        if (e != cudaSuccess) return cuda_fail(e, "kernel load");
+    }
+    return LUSP_OK;
+}
+
 int refactor_occupancy(int prec, size_t smem, int block, int* occ) {
     if (prec == LUSP_FP64) return refactor_prepare<double>(smem, block, occ);
     return refactor_prepare<float>(smem, block, occ);

@@ -137,6 +137,9 @@ char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m)
 size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& rplan);
 int launch_systems(const LaunchArgs& a, cudaStream_t st);
 int sm_count();
+// Loads every engine kernel into the current context now (not lazily at
+// its first launch).
+int preload_kernels();
 void batch_free(BatchObj* B);
 int batch_launch(BatchObj* B, int what, cudaStream_t st);
 

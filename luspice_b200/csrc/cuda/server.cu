@@ -101,6 +101,9 @@ struct ServerObj {
     std::deque<Request*> queue;                       // waiting for a launch
     std::unordered_multimap<uint64_t, std::unique_ptr<PatternEntry>> patterns;
     std::deque<PatternEntry*> analysis_q;
+    // Device patterns to free.  cudaFree waits for the whole device, so the
+    // analysis threads free them outside the lock, never the scheduler.
+    std::vector<PatternObj*> to_free;
     std::vector<Flight> flights;
     size_t pattern_bytes = 0, pattern_budget = 0;
     lusp_server_stats stats{};
@@ -120,6 +123,10 @@ struct ServerObj {
 
 int ServerObj::init() {
     cudaGetDevice(&device);
+    // Every kernel a request may need (the fp64 rungs included) is loaded
+    // before the first request, not in the middle of the stream.
+    int prc = preload_kernels();
+    if (prc != LUSP_OK) return prc;
     const int ns = std::max(1, opts.streams);
     flights.resize(ns);
     const size_t arena = (size_t)(opts.arena_gb * 1e9);
@@ -169,18 +176,29 @@ void ServerObj::shutdown() {
     }
     for (auto& kv : patterns)
         if (kv.second->pat) pattern_free(kv.second->pat);
+    for (PatternObj* P : to_free) pattern_free(P);
+    to_free.clear();
 }
 
 void ServerObj::analysis_loop() {
     cudaSetDevice(device);
     while (true) {
         PatternEntry* pe = nullptr;
+        std::vector<PatternObj*> frees;
         {
             std::unique_lock<std::mutex> lk(mu);
-            cv_analysis.wait(lk, [this] { return stopping || !analysis_q.empty(); });
-            if (analysis_q.empty()) return;
-            pe = analysis_q.front();
-            analysis_q.pop_front();
+            cv_analysis.wait(lk, [this] { return stopping || !analysis_q.empty() || !to_free.empty(); });
+            frees.swap(to_free);
+            if (!analysis_q.empty()) {
+                pe = analysis_q.front();
+                analysis_q.pop_front();
+            }
+        }
+        for (PatternObj* P : frees) pattern_free(P);
+        if (!pe) {
+            std::lock_guard<std::mutex> lk(mu);
+            if (stopping && analysis_q.empty()) return;
+            continue;
         }
         PatternObj* P = nullptr;
         const int rc = pattern_build(pe->n, pe->Ap.data(), pe->Ai.data(), pe->Ax.data(), nullptr, &P);
@@ -214,7 +232,8 @@ void ServerObj::release(PatternEntry* pe) {
         if (it->second.get() != pe) continue;
         if (pe->pat) {
             pattern_bytes -= pe->pat->bytes;
-            pattern_free(pe->pat);
+            to_free.push_back(pe->pat);
+            cv_analysis.notify_one();
             stats.patterns_resident--;
         }
         patterns.erase(it);
@@ -238,7 +257,8 @@ void ServerObj::evict_if_needed() {
         }
         if (!victim) return;
         pattern_bytes -= victim->pat->bytes;
-        pattern_free(victim->pat);
+        to_free.push_back(victim->pat);
+        cv_analysis.notify_one();
         patterns.erase(vit);
         stats.evictions++;
         stats.patterns_resident--;
