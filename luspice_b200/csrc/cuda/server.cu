@@ -101,8 +101,8 @@ struct ServerObj {
     std::deque<Request*> queue;                       // waiting for a launch
     std::unordered_multimap<uint64_t, std::unique_ptr<PatternEntry>> patterns;
     std::deque<PatternEntry*> analysis_q;
-    // Device patterns to free.  cudaFree waits for the whole device, so the
-    // analysis threads free them outside the lock, never the scheduler.
+    // Device patterns to free.  cudaFree waits for the whole device, so they
+    // are freed only when no launch is in flight (the scheduler, idle).
     std::vector<PatternObj*> to_free;
     std::vector<Flight> flights;
     size_t pattern_bytes = 0, pattern_budget = 0;
@@ -184,21 +184,12 @@ void ServerObj::analysis_loop() {
     cudaSetDevice(device);
     while (true) {
         PatternEntry* pe = nullptr;
-        std::vector<PatternObj*> frees;
         {
             std::unique_lock<std::mutex> lk(mu);
-            cv_analysis.wait(lk, [this] { return stopping || !analysis_q.empty() || !to_free.empty(); });
-            frees.swap(to_free);
-            if (!analysis_q.empty()) {
-                pe = analysis_q.front();
-                analysis_q.pop_front();
-            }
-        }
-        for (PatternObj* P : frees) pattern_free(P);
-        if (!pe) {
-            std::lock_guard<std::mutex> lk(mu);
-            if (stopping && analysis_q.empty()) return;
-            continue;
+            cv_analysis.wait(lk, [this] { return stopping || !analysis_q.empty(); });
+            if (analysis_q.empty()) return;
+            pe = analysis_q.front();
+            analysis_q.pop_front();
         }
         PatternObj* P = nullptr;
         const int rc = pattern_build(pe->n, pe->Ap.data(), pe->Ai.data(), pe->Ax.data(), nullptr, &P);
@@ -233,7 +224,6 @@ void ServerObj::release(PatternEntry* pe) {
         if (pe->pat) {
             pattern_bytes -= pe->pat->bytes;
             to_free.push_back(pe->pat);
-            cv_analysis.notify_one();
             stats.patterns_resident--;
         }
         patterns.erase(it);
@@ -258,7 +248,6 @@ void ServerObj::evict_if_needed() {
         if (!victim) return;
         pattern_bytes -= victim->pat->bytes;
         to_free.push_back(victim->pat);
-        cv_analysis.notify_one();
         patterns.erase(vit);
         stats.evictions++;
         stats.patterns_resident--;
@@ -586,6 +575,11 @@ void ServerObj::sched_loop() {
         if (progress) cv_done.notify_all();
         bool busy = false;
         for (auto& f : flights) busy |= f.busy;
+        if (!busy && !to_free.empty()) {
+            // Nothing in flight: a free here waits for no kernel.
+            for (PatternObj* P : to_free) pattern_free(P);
+            to_free.clear();
+        }
         if (stopping && !busy && queue.empty()) return;
         if (!progress) {
             // Poll completions every 20 us while work is in flight; sleep
