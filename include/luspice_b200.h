@@ -228,6 +228,13 @@ int lusp_batch_factor_device_ptr(lusp_batch *b, int sys, void **d_values);
 int lusp_batch_set_params(lusp_batch *b, const lusp_batch_opts *opts);
 /* Kernel launches issued by the last lusp_batch_run (for accounting). */
 int lusp_batch_launch_count(const lusp_batch *b);
+/* on != 0: later lusp_batch_run calls (not graph replays) record CUDA events
+ * on their stream around the refactor, dense-block and solve kernels;
+ * lusp_batch_kernel_ms then waits for the last such run and returns the
+ * three kernels' device times in ms (0 for a kernel that run did not
+ * launch; LUSP_EARG while timing is off). */
+int lusp_batch_time_kernels(lusp_batch *b, int on);
+int lusp_batch_kernel_ms(lusp_batch *b, float *ms3);
 
 /* ---- serving loop ----
  * Continuous batching of refactor+solve requests from concurrent callers

@@ -136,6 +136,8 @@ SIGNATURES = {
     "lusp_batch_factor_device_ptr": (C.c_int, [C.c_void_p, C.c_int, c_void_pp]),
     "lusp_batch_set_params": (C.c_int, [C.c_void_p, C.POINTER(BatchOpts)]),
     "lusp_batch_launch_count": (C.c_int, [C.c_void_p]),
+    "lusp_batch_time_kernels": (C.c_int, [C.c_void_p, C.c_int]),
+    "lusp_batch_kernel_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "lusp_sell_create": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, C.c_int, C.c_int,
                                    C.c_int, c_void_pp]),
     "lusp_sell_destroy": (None, [C.c_void_p]),

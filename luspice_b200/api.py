@@ -193,6 +193,18 @@ class Batch:
     def launch_count(self) -> int:
         return L.load().lusp_batch_launch_count(self.handle)
 
+    def time_kernels(self, on: bool = True) -> None:
+        """Record CUDA events around each kernel of later run() calls
+        (graph=False)."""
+        _check(L.load().lusp_batch_time_kernels(self.handle, int(on)), "time_kernels")
+
+    def kernel_ms(self) -> dict:
+        """Device times (ms) of the last timed run's refactor, dense-block and
+        solve kernels."""
+        ms = (C.c_float * 3)()
+        _check(L.load().lusp_batch_kernel_ms(self.handle, ms), "kernel_ms")
+        return {"refactor": ms[0], "dense": ms[1], "solve": ms[2]}
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             L.load().lusp_batch_destroy(self.handle)

@@ -222,7 +222,7 @@ int lusp_batch_download(lusp_batch* hb, double* x, void* stream) {
 int lusp_batch_run(lusp_batch* hb, int what, void* stream) {
     BatchObj* B = BO(hb);
     if (!B || (what & 3) == 0 || what > 7) return LUSP_EARG;
-    return lusp::batch_launch(B, what, (cudaStream_t)stream);
+    return lusp::batch_launch(B, what, (cudaStream_t)stream, true);
 }
 
 int lusp_batch_run_graph(lusp_batch* hb, int what, void* stream) {
@@ -328,6 +328,32 @@ int lusp_batch_set_params(lusp_batch* hb, const lusp_batch_opts* o) {
 int lusp_batch_launch_count(const lusp_batch* hb) {
     const BatchObj* B = BO(hb);
     return B ? B->launches : 0;
+}
+
+int lusp_batch_time_kernels(lusp_batch* hb, int on) {
+    BatchObj* B = BO(hb);
+    if (!B) return LUSP_EARG;
+    if (on && !B->kev[0]) {
+        for (cudaEvent_t& ev : B->kev) {
+            cudaError_t e = cudaEventCreate(&ev);
+            if (e != cudaSuccess) return lusp::cuda_fail(e, "timing events");
+        }
+    } else if (!on && B->kev[0]) {
+        for (cudaEvent_t& ev : B->kev) {
+            cudaEventDestroy(ev);
+            ev = nullptr;
+        }
+    }
+    return LUSP_OK;
+}
+
+int lusp_batch_kernel_ms(lusp_batch* hb, float* ms) {
+    BatchObj* B = BO(hb);
+    if (!B || !ms || !B->kev[0]) return LUSP_EARG;
+    cudaError_t e = cudaEventSynchronize(B->kev[3]);
+    for (int k = 0; k < 3 && e == cudaSuccess; k++) e = cudaEventElapsedTime(ms + k, B->kev[k], B->kev[k + 1]);
+    if (e != cudaSuccess) return lusp::cuda_fail(e, "kernel times");
+    return LUSP_OK;
 }
 
 }  // extern "C"

@@ -596,10 +596,14 @@ static RungShape ladder_shape(const LaunchArgs& a) {
 // Refactor, dense-block and solve kernels of one rung over sys[0, nsys) (or
 // the dyn / list items) with the work counters q[0..2].
 template <typename VT, typename AT>
+// kev (may be null): four events recorded on st around the kernels: before
+// the refactor kernel, between it and the dense-block kernel, between that
+// and the solve kernel, after the solve kernel.
 static int launch_rung(const SysDev* sys, int nsys, int* q, const int* dyn, const int* list, int what,
                        const RungShape& r, const SolveParams& prm, int direct, const EscDev& esc, int rung,
-                       cudaStream_t st) {
+                       cudaStream_t st, cudaEvent_t* kev = nullptr) {
     cudaError_t e;
+    if (kev && cudaEventRecord(kev[0], st) != cudaSuccess) return cuda_fail(cudaGetLastError(), "timing event");
     if (what & LUSP_RUN_REFACTOR) {
         int rc = refactor_prepare<VT>(r.rplan.bytes, r.rblock, nullptr);
         if (rc != LUSP_OK) return rc;
@@ -623,6 +627,7 @@ static int launch_rung(const SysDev* sys, int nsys, int* q, const int* dyn, cons
             e = cudaGetLastError();
         }
         if (e != cudaSuccess) return cuda_fail(e, "refactor kernel launch");
+        if (kev && cudaEventRecord(kev[1], st) != cudaSuccess) return cuda_fail(cudaGetLastError(), "timing event");
         if (r.dgrid > 0) {
             rc = dense_prepare<VT>(r.dplan.bytes, r.dblock, nullptr);
             if (rc != LUSP_OK) return rc;
@@ -630,7 +635,10 @@ static int launch_rung(const SysDev* sys, int nsys, int* q, const int* dyn, cons
             e = cudaGetLastError();
             if (e != cudaSuccess) return cuda_fail(e, "dense kernel launch");
         }
+    } else if (kev && cudaEventRecord(kev[1], st) != cudaSuccess) {
+        return cuda_fail(cudaGetLastError(), "timing event");
     }
+    if (kev && cudaEventRecord(kev[2], st) != cudaSuccess) return cuda_fail(cudaGetLastError(), "timing event");
     if (what & LUSP_RUN_SOLVE) {
         int rc = kernel_prepare<VT, AT>(r.plan.bytes, r.block, nullptr);
         if (rc != LUSP_OK) return rc;
@@ -639,6 +647,7 @@ static int launch_rung(const SysDev* sys, int nsys, int* q, const int* dyn, cons
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "solve kernel launch");
     }
+    if (kev && cudaEventRecord(kev[3], st) != cudaSuccess) return cuda_fail(cudaGetLastError(), "timing event");
     return LUSP_OK;
 }
 
@@ -650,7 +659,7 @@ static int launch_typed(const LaunchArgs& a, cudaStream_t st) {
     const bool ladder = a.rungs != 0 && a.prec != LUSP_FP64 && !direct && (a.what & LUSP_RUN_SOLVE);
     EscDev none{};
     int rc = launch_rung<VT, AT>(a.d_sys, a.nsys, a.d_queue, nullptr, nullptr, a.what, main_shape(a), a.prm, direct,
-                                 ladder ? a.esc : none, 0, st);
+                                 ladder ? a.esc : none, 0, st, a.kev);
     if (rc != LUSP_OK || !ladder) return rc;
     // The fp64 rungs: every kernel reads its item count from the slot
     // counters the solve kernels above wrote (no host round trip).
@@ -688,9 +697,10 @@ int launch_kernel_count(const LaunchArgs& a, int what) {
     return n;
 }
 
-int batch_launch(BatchObj* B, int what, cudaStream_t st) {
+int batch_launch(BatchObj* B, int what, cudaStream_t st, bool timed) {
     LaunchArgs a = B->launch;
     a.what = what;
+    a.kev = timed && B->kev[0] ? B->kev : nullptr;
     int rc = launch_systems(a, st);
     if (rc == LUSP_OK) B->launches = launch_kernel_count(a, what);
     return rc;
@@ -988,6 +998,8 @@ void batch_free(BatchObj* B) {
     }
     if (B->d_block) cudaFree(B->d_block);
     if (B->d_ladder) cudaFree(B->d_ladder);
+    for (cudaEvent_t ev : B->kev)
+        if (ev) cudaEventDestroy(ev);
     delete B;
 }
 

@@ -34,6 +34,7 @@ struct LaunchArgs {
     int inner = 0;
     int what = LUSP_RUN_BOTH;
     int ir64 = 0;                    // fp64 factors solved by GMRES-IR, not directly
+    cudaEvent_t* kev = nullptr;      // per-kernel timing events of the main rung (or null)
     int block = 256;
     int grid = 1;
     SmemPlan rplan{};                // refactorization kernel
@@ -99,6 +100,7 @@ struct BatchObj {
     int block = 256;
     int grid = 1;
     int launches = 0;
+    cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};   // per-kernel timing (lusp_batch_time_kernels)
     LaunchArgs launch{};
     std::map<std::pair<int, cudaStream_t>, GraphEntry> graphs;
 };
@@ -141,7 +143,9 @@ int sm_count();
 // its first launch).
 int preload_kernels();
 void batch_free(BatchObj* B);
-int batch_launch(BatchObj* B, int what, cudaStream_t st);
+// timed: record the per-kernel timing events when the batch has them (not
+// in graph capture).
+int batch_launch(BatchObj* B, int what, cudaStream_t st, bool timed = false);
 
 }  // namespace lusp
 

@@ -103,6 +103,37 @@ def test_graph_replay_matches(gpu):
     assert np.array_equal(x0, x1)
 
 
+def test_kernel_timing_events(gpu):
+    """Per-kernel CUDA-event times of a run: all three kernels timed, they add
+    up to no more than the whole run, the results equal an untimed run's,
+    and a refactor-only run reports no solve time."""
+    import torch
+    m = mna.power_grid(15, 16, 6, seed=3)
+    P = api.Pattern.from_matrix(m, dense_tail=64)
+    vals = m.perturbed(3, seed=2)
+    B = api.Batch([P] * 3)
+    B.upload(list(vals), [m.b] * 3)
+    B.run(api.RUN_BOTH)
+    x0 = B.download().copy()
+    with pytest.raises(api.LuspError):
+        B.kernel_ms()
+    B.time_kernels(True)
+    s = torch.cuda.Stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    B.run(api.RUN_BOTH, stream=s)
+    b.record(s)
+    t = B.kernel_ms()
+    torch.cuda.synchronize()
+    assert t["refactor"] > 0 and t["dense"] > 0 and t["solve"] > 0
+    assert t["refactor"] + t["dense"] + t["solve"] <= a.elapsed_time(b) + 1e-3
+    assert np.array_equal(B.download(), x0)
+    B.run(api.RUN_REFACTOR)
+    t = B.kernel_ms()
+    assert t["refactor"] > 0 and t["solve"] < 0.01
+    B.time_kernels(False)
+
+
 def test_direct_solve_fp32_factors(gpu):
     m = mna.analog(400, 9)
     P = api.Pattern.from_matrix(m)
