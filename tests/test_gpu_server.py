@@ -126,3 +126,81 @@ def test_repivot_when_frozen_pivot_vanishes(gpu):
     st = S.stats()
     assert st["patterns_resident"] == 1     # the request's own analysis is gone
     S.close()
+
+
+def test_oversized_request_refused_others_served(gpu):
+    """A request whose inputs exceed a stream's staging area completes at once
+    with LUSP_EALLOC and the capacity status; requests around it are served."""
+    small = mna.analog(300, 3)
+    big = mna.large_circuit(3000, seed=5)
+    S = api.Server(max_batch=8, streams=1, arena_gb=0.5, staging_mb=0.1)
+    i0 = S.submit(small.n, small.Ap, small.Ai, small.Ax, small.b)
+    i1 = S.submit(big.n, big.Ap, big.Ai, big.Ax, big.b)
+    i2 = S.submit(small.n, small.Ap, small.Ai, small.Ax, small.b)
+    _, r1 = S.poll(i1, 120000)
+    assert r1["rc"] == 2 and r1["status"] & api.ST_CAPACITY, r1
+    for i in (i0, i2):
+        x, r = S.poll(i, 120000)
+        assert r["rc"] == 0
+        assert rel_err(x, oracle_solution(small, small.Ax)) <= TOL_REL
+    S.close()
+
+
+def test_many_concurrent_submitters(gpu):
+    """Eight threads submit and poll their own requests over three patterns:
+    every request completes with the oracle's answer and the counters add up."""
+    mats = [mna.analog(n, 40 + n) for n in (200, 600, 1200)]
+    S = api.Server(max_batch=32, streams=3, arena_gb=0.5, staging_mb=32)
+    errors, lock = [], threading.Lock()
+
+    def worker(k):
+        for t in range(12):
+            m = mats[(k + t) % 3]
+            v = m.perturbed(1, seed=100 * k + t)[0]
+            x, r = S.poll(S.submit(m.n, m.Ap, m.Ai, v, m.b), 120000)
+            if r["rc"] != 0 or rel_err(x, oracle_solution(m, v)) > TOL_REL:
+                with lock:
+                    errors.append((k, t, r))
+
+    th = [threading.Thread(target=worker, args=(k,)) for k in range(8)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errors, errors[:3]
+    st = S.stats()
+    assert st["submitted"] == st["completed"] == 96
+    assert st["cache_misses"] == 3 and st["cache_hits"] == 93
+    S.close()
+
+
+def test_escalation_off_keeps_the_failed_result(gpu):
+    """escalate = 0: a system whose mixed solve fails is returned as it is,
+    with its failure status and no escalation."""
+    m = mna.analog(989, 42)
+    S = api.Server(max_batch=4, streams=1, arena_gb=0.5, staging_mb=32, escalate=0, rtol=1e-300)
+    _, r = S.poll(S.submit(m.n, m.Ap, m.Ai, m.Ax, m.b), 120000)
+    assert r["rc"] == 0 and not r["escalated"]
+    assert r["status"] & (api.ST_NOT_CONVERGED | api.ST_STAGNATED)
+    assert S.stats()["escalated"] == 0
+    S.close()
+
+
+def test_lru_eviction_and_reanalysis(gpu):
+    """A pattern budget of a few MB beside the arena: older patterns leave the
+    device, and a pattern seen again after its eviction is analysed again and
+    still gives the oracle's answer."""
+    mats = [mna.analog(1500, 60 + i) for i in range(6)]
+    arena = 0.25
+    S = api.Server(max_batch=4, streams=1, arena_gb=arena, staging_mb=32, hbm_budget_gb=arena + 0.004)
+    for m in mats:
+        x, r = S.poll(S.submit(m.n, m.Ap, m.Ai, m.Ax, m.b), 120000)
+        assert r["rc"] == 0
+    st = S.stats()
+    assert st["evictions"] > 0 and st["pattern_gb"] <= 0.004 + 1e-9, st
+    m = mats[0]
+    v = m.perturbed(1, seed=3)[0]
+    x, r = S.poll(S.submit(m.n, m.Ap, m.Ai, v, m.b), 120000)
+    assert r["rc"] == 0 and not r["cache_hit"]
+    assert rel_err(x, oracle_solution(m, v)) <= TOL_REL
+    S.close()
