@@ -103,25 +103,16 @@ int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
     }
 
     std::vector<int> col_w(n_col, 1);
+    // Weighted live degree of every row.  It never changes while the row is
+    // alive: a column is ordered only together with all its rows (they die
+    // into the new pivot row), and merging a supercolumn moves weight
+    // between two columns that share all their rows.
+    std::vector<int> row_w(n_row);
+    for (int r = 0; r < n_row; r++) row_w[r] = (int)row_cols[r].size();
     std::vector<std::vector<int>> members(n_col);
     int remaining = 0;
     for (int c = 0; c < n_col; c++)
         if (cstate[c] == LIVE) { members[c].push_back(c); remaining++; }
-
-    // Weighted live degree of a row; compacts the row's column list.
-    auto row_weight = [&](int r) {
-        auto& v = row_cols[r];
-        int w = 0;
-        size_t o = 0;
-        for (size_t t = 0; t < v.size(); t++) {
-            const int c = v[t];
-            if (cstate[c] != LIVE) continue;
-            v[o++] = c;
-            w += col_w[c];
-        }
-        v.resize(o);
-        return w;
-    };
 
     Buckets bk(n_col);
     for (int c = 0; c < n_col; c++) {
@@ -170,11 +161,12 @@ int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
             v.erase(std::remove_if(v.begin(), v.end(), [&](int r) { return !row_alive[r]; }), v.end());
             v.push_back(e);
         }
+        row_w.push_back(wP);
         // |r \ pivot row| for every row meeting the pivot row's columns.
         for (int j : pivrow)
             for (int r : col_rows[j]) {
                 if (r == e) continue;
-                if (rtag[r] != tag) { rtag[r] = tag; rdiff[r] = row_weight(r); }
+                if (rtag[r] != tag) { rtag[r] = tag; rdiff[r] = row_w[r]; }
                 rdiff[r] -= col_w[j];
             }
         for (int j : pivrow) {
