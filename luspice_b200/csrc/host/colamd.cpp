@@ -71,12 +71,13 @@ int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
     std::vector<std::vector<int>> col_rows(n_col);
     for (int c = 0; c < n_col; c++) {
         auto& v = col_rows[c];
+        v.reserve(Ap[c + 1] - Ap[c] + 4);
         for (int p = Ap[c]; p < Ap[c + 1]; p++) {
             const int r = Ai[p];
             if (r < 0 || r >= n_row) return -2;
             v.push_back(r);
         }
-        std::sort(v.begin(), v.end());
+        if (!std::is_sorted(v.begin(), v.end())) std::sort(v.begin(), v.end());
         v.erase(std::unique(v.begin(), v.end()), v.end());
     }
     std::vector<unsigned char> cstate(n_col, LIVE);
@@ -126,6 +127,7 @@ int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
     std::vector<int> order;
     order.reserve(n_col);
     std::vector<int> cmark(n_col, 0), pivrow;
+    std::vector<std::pair<unsigned long long, int>> hs;
     std::vector<int> rtag(n_row, 0), rdiff(n_row, 0);
     int tag = 0;
 
@@ -180,11 +182,12 @@ int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
         }
         // Supercolumns: identical row sets among the pivot row's columns.
         if (pivrow.size() > 1) {
-            std::vector<std::pair<unsigned long long, int>> hs;
-            hs.reserve(pivrow.size());
+            hs.clear();
             for (int j : pivrow) {
                 auto& v = col_rows[j];
-                std::sort(v.begin(), v.end());
+                // Already ascending in practice (a new pivot row carries the
+                // largest row index so far and erasing keeps the order).
+                if (!std::is_sorted(v.begin(), v.end())) std::sort(v.begin(), v.end());
                 unsigned long long h = v.size();
                 for (int r : v) h = h * 1000003ull + (unsigned)r;
                 hs.emplace_back(h, j);
