@@ -507,10 +507,10 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
                 tmp.emplace_back((int)(it - rb), p);
                 if (Ai[p] == c) S.a_diag[k] = (int)(it - rb);
             }
-            std::stable_sort(tmp.begin(), tmp.end(),
-                             [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
-                                 return a.first < b.first;
-                             });
+            // By slot, input order within a slot (the second members are the
+            // input positions, ascending as appended, so sorting the pairs is
+            // the stable order without a merge buffer).
+            std::sort(tmp.begin(), tmp.end());
             int o = S.a_ptr[k];
             for (auto& e : tmp) {
                 S.a_dst[o] = e.first;
