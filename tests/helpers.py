@@ -7,7 +7,7 @@ import numpy as np
 from luspice_b200 import api, mna
 from oracle import oracle as O
 
-TOL_REL = 1e-6          # north-star acceptance: rel-L2 error vs the fp64 oracle
+TOL_REL = 1e-6          # acceptance: rel-L2 error vs the fp64 oracle
 
 
 def a_slot_map(m, pattern):
