@@ -87,7 +87,17 @@ int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
         else if ((int)col_rows[c].size() > dense_col) { cstate[c] = DENSE; dense_cols.push_back(c); }
     }
 
-    std::vector<std::vector<int>> row_cols(n_row);
+    // Rows: one vector per original row plus one per pivot row to come.
+    std::vector<std::vector<int>> row_cols;
+    row_cols.reserve((size_t)n_row + n_col);
+    row_cols.resize(n_row);
+    {
+        std::vector<int> cnt(n_row, 0);
+        for (int c = 0; c < n_col; c++)
+            if (cstate[c] == LIVE)
+                for (int r : col_rows[c]) cnt[r]++;
+        for (int r = 0; r < n_row; r++) row_cols[r].reserve(cnt[r]);
+    }
     for (int c = 0; c < n_col; c++)
         if (cstate[c] == LIVE)
             for (int r : col_rows[c]) row_cols[r].push_back(c);
@@ -110,10 +120,12 @@ int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
     // between two columns that share all their rows.
     std::vector<int> row_w(n_row);
     for (int r = 0; r < n_row; r++) row_w[r] = (int)row_cols[r].size();
-    std::vector<std::vector<int>> members(n_col);
+    // Members of each supercolumn, a linked list in merge order.
+    std::vector<int> mnext(n_col, -1), mtail(n_col);
+    for (int c = 0; c < n_col; c++) mtail[c] = c;
     int remaining = 0;
     for (int c = 0; c < n_col; c++)
-        if (cstate[c] == LIVE) { members[c].push_back(c); remaining++; }
+        if (cstate[c] == LIVE) remaining++;
 
     Buckets bk(n_col);
     for (int c = 0; c < n_col; c++) {
@@ -129,6 +141,10 @@ int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
     std::vector<int> cmark(n_col, 0), pivrow;
     std::vector<std::pair<unsigned long long, int>> hs;
     std::vector<int> rtag(n_row, 0), rdiff(n_row, 0);
+    rtag.reserve((size_t)n_row + n_col);
+    rdiff.reserve((size_t)n_row + n_col);
+    row_alive.reserve((size_t)n_row + n_col);
+    row_w.reserve((size_t)n_row + n_col);
     int tag = 0;
 
     while (remaining > 0) {
@@ -204,8 +220,8 @@ int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
                         if (cstate[j2] != LIVE) continue;
                         if (col_rows[j1] != col_rows[j2]) continue;
                         col_w[j1] += col_w[j2];
-                        members[j1].insert(members[j1].end(), members[j2].begin(), members[j2].end());
-                        members[j2].clear();
+                        mnext[mtail[j1]] = j2;
+                        mtail[j1] = mtail[j2];
                         cstate[j2] = MERGED;
                         bk.remove(j2);
                         col_rows[j2].clear();
@@ -218,7 +234,7 @@ int colamd_order(int n_row, int n_col, const int* Ap, const int* Ai,
 
     int pos = 0;
     for (int c : order)
-        for (int m : members[c]) q_out[pos++] = m;
+        for (int m = c; m >= 0; m = mnext[m]) q_out[pos++] = m;
     for (int c : dense_cols) q_out[pos++] = c;
     for (int c : empty_cols) q_out[pos++] = c;
     return pos == n_col ? 0 : -3;
