@@ -3,20 +3,26 @@
 Workload (one step): the 63x64 power-grid MNA matrix plus 18 Vdd pad rows
 (n = 4050), 50 Newton refactorizations on the same pattern with element
 values perturbed log-normally (sigma = 0.1), each followed by a full solve:
-fp32 factors (frozen pivots) + fp64 GMRES-IR (restart 30, inner stop 1e-4, rtol 1e-10), all
-50 systems in one CUDA graph of three persistent kernels (sparse refactor,
-dense trailing block, solve).  `value` counts only systems whose
-solution is within rel-L2 1e-6 of the fp64 oracle (checked after timing).
+fp32 factors (frozen pivots) + fp64 GMRES-IR (restart 30, inner stop 1e-4,
+rtol 1e-10), all 50 systems in one CUDA graph of the engine's persistent
+kernels.  `value` counts only systems whose solution is within rel-L2 1e-6
+of the fp64 oracle (the compiled reference's solve, checked after timing).
 
-Also reported: the plain fp64 GPU path on the same inputs (per request and
-batched), p50/p99 single-request latency, the end-to-end figure through the
-public API with host buffers (e2e), the roofline of the solve kernel, and
-the reference's CPU path (cpu_baseline).
+Also reported on the same line: the plain fp64 GPU path on the same inputs
+and the same timing protocol (batched; per request), p50/p99 single-request
+latency, the end-to-end figure through the public API with host buffers
+(e2e), the roofline of the sparse refactor kernel (the dominant kernel) and
+of the solve kernel, the reference's CPU path on one pinned core
+(cpu_baseline), and the other workloads as keys: config0 (n = 989 analog
+circuit: CPU factor+solve time, GPU per request and batched), config2 (512
+uneven analog matrices x 8 refactors in one launch) and config3 (n = 40,000
+circuit: SpMV variants and the full solve).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 For N > 1 launch with torch.distributed.run (one rank per GPU); ranks run
 independent replicas of the workload (no exchange), value = all ranks'
-systems / max time.
+systems / max time.  --impl reference times the reference's CPU path over
+all host cores on the same value sets (rank 0 only).
 """
 from __future__ import annotations
 
@@ -41,8 +47,9 @@ NSYS = 50
 # the host has queued the timed work before the GPU reaches it.
 HOST_AHEAD_CYCLES = 200_000
 WORKLOAD = ("power-grid MNA n=4050 (63x64 mesh + 18 Vdd pads), 50 Newton refactors on one "
-            "pattern (log-normal sigma=0.1 element perturbation), fp32 factor + fp64 GMRES-IR "
-            "(restart 30, inner stop 1e-4, rtol 1e-10, forward-error stop 1e-8), one graph of three persistent kernels per step")
+            "pattern (log-normal sigma=0.1 element perturbation), each followed by a full solve")
+METHOD = ("fp32 factor (frozen pivots, fp64 work vector) + fp64 GMRES-IR (restart 30, inner stop 1e-4, "
+          "rtol 1e-10, forward-error stop 1e-8); one CUDA graph of the engine's kernels per step")
 
 
 def peaks():
@@ -141,38 +148,82 @@ def algorithmic_bytes(info, stats, vs=4):
     return total_ref, total
 
 
-def ref_cpu_worker(args):
-    """One reference CPU factor+solve (compiled reference sources)."""
-    n, Ap, Ai, vals, q, b = args
-    from oracle import oracle
-    t = time.perf_counter()
-    x = oracle.ref_cpu_solve(n, Ap, Ai, vals, q, b)
-    return time.perf_counter() - t, x
+def host_cpu():
+    """Host CPU description for the CPU legs: model, logical cores, cores
+    this process may run on."""
+    model = "unknown"
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count(), "allowed": len(os.sched_getaffinity(0))}
 
 
-def cpu_reference_rate(m, vals, q, threads, budget_s=12.0):
-    """Reference CPU path (splu lu_factor + lu_solve_perm, cpu_ref_lu.c) on a
-    bounded sample of the same value sets; returns (systems/s, sample desc, kind)."""
+def cpu_pinned_pass_times(units, repeats=5, budget_s=None):
+    """The reference CPU path (one lu_factor + one lu_solve_perm per unit,
+    src/cpu_ref_lu.c:15-58, compiled from the reference's sources) run on ONE
+    pinned core: one untimed unit, then `repeats` timed passes over the
+    units.  Returns (seconds per pass for each pass, the core, kind)."""
     from oracle import oracle
     kind = "reference" if oracle.ref_available() else "port"
-    work = [(m.n, m.Ap, m.Ai, vals[i % len(vals)], q, m.b) for i in range(len(vals))]
-    if threads <= 1:
-        done, t0 = 0, time.perf_counter()
-        while time.perf_counter() - t0 < budget_s:
-            ref_cpu_worker(work[done % len(work)])
-            done += 1
-        el = time.perf_counter() - t0
-        return done / el, f"{done} refactor+solves of the step's value sets, 1 thread, {el:.1f} s", kind
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(threads) as pool:
-        pool.map(ref_cpu_worker, work[:threads])  # warm the workers
-        done, t0 = 0, time.perf_counter()
-        while time.perf_counter() - t0 < budget_s:
-            pool.map(ref_cpu_worker, work)
-            done += len(work)
-        el = time.perf_counter() - t0
-    return done / el, f"{done} refactor+solves of the step's value sets, {threads} processes, {el:.1f} s", kind
+    allowed = sorted(os.sched_getaffinity(0))
+    core = allowed[-1]
+    old = set(allowed)
+    os.sched_setaffinity(0, {core})
+    try:
+        oracle.ref_cpu_solve(*units[0])
+        ts = []
+        t_all = time.perf_counter()
+        for _ in range(repeats):
+            t = time.perf_counter()
+            for u in units:
+                oracle.ref_cpu_solve(*u)
+            ts.append(time.perf_counter() - t)
+            if budget_s is not None and len(ts) >= 5 and time.perf_counter() - t_all > budget_s:
+                break
+    finally:
+        os.sched_setaffinity(0, old)
+    return ts, core, kind
+
+
+def cpu_baseline_1core(m, vals, q, repeats=5):
+    """cpu_baseline of the default line: the step's value sets, one core."""
+    units = [(m.n, m.Ap, m.Ai, v, q, m.b) for v in vals]
+    ts, core, kind = cpu_pinned_pass_times(units, repeats)
+    med, mn = statistics.median(ts), min(ts)
+    return {"value": len(units) / med, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{len(units)} refactor+solves (the step's value sets, one lu_factor + one "
+                      f"lu_solve_perm each) per pass, {len(ts)} passes on core {core} (pinned); value from "
+                      f"the median pass {1000 * med:.1f} ms, best pass {1000 * mn:.1f} ms",
+            "best_value": len(units) / mn, "cpu": host_cpu()}
+
+
+_REF_WORK = None
+
+
+def _ref_pool_init(counter, cores, work):
+    """Pool worker set-up: pin to the next free core, keep the workload."""
+    global _REF_WORK
+    with counter.get_lock():
+        i = counter.value
+        counter.value += 1
+    os.sched_setaffinity(0, {cores[i % len(cores)]})
+    _REF_WORK = work
+
+
+def _ref_pool_unit(i):
+    from oracle import oracle
+    n, Ap, Ai, vals, q, b = _REF_WORK
+    return oracle.ref_cpu_solve(n, Ap, Ai, vals[i % len(vals)], q, b) is not None
+
+
+def workload_config(m, world):
+    """The `config` of both arms (the driver compares them)."""
+    return {"workload": WORKLOAD, "systems_per_step": NSYS, "n": m.n, "nnz": m.nnz,
+            "parallelism": f"replicas x{world}"}
 
 
 def setup_dist(n_gpus):
@@ -198,22 +249,49 @@ def barrier(world):
 
 
 def run_reference(args):
-    rank, world, local = setup_dist(args.gpus)
+    """The reference's CPU path (lu_factor + lu_solve_perm compiled from its
+    sources) over all host cores, one pinned worker process per core, on the
+    same value sets and column order as the GPU arm.  A step = the step's 50
+    refactor+solves.  This process loads only the checker libraries: the
+    column order comes from oracle/power_grid_colamd_q.npy (the reference has
+    no COLAMD), the matrix from the pure-Python generator."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from luspice_b200 import api, mna
+    import multiprocessing as mp
+    from luspice_b200 import mna
     from oracle import oracle
     m = mna.power_grid()
     vals = m.perturbed(NSYS, seed=4242)
-    q = api.colamd(m.n, m.Ap, m.Ai)
-    threads = os.cpu_count() or 1
-    rate, sample, kind = cpu_reference_rate(m, vals, q, threads, budget_s=max(3.0, 2.0 * args.steps))
-    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * NSYS / rate,
+    q = np.load(ROOT / "oracle" / "power_grid_colamd_q.npy")
+    cores = sorted(os.sched_getaffinity(0))
+    kind = "reference" if oracle.ref_available() else "port"
+    ctx = mp.get_context("spawn")
+    counter = ctx.Value("i", 0)
+    work = (m.n, m.Ap, m.Ai, vals, q, m.b)
+    with ctx.Pool(len(cores), initializer=_ref_pool_init, initargs=(counter, cores, work)) as pool:
+        for _ in range(max(args.warmup, 1)):
+            assert all(pool.map(_ref_pool_unit, range(NSYS), chunksize=1))
+        ts = []
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            pool.map(_ref_pool_unit, range(NSYS), chunksize=1)
+            ts.append(time.perf_counter() - t)
+    total = sum(ts)
+    rate = NSYS * len(ts) / total
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / len(ts),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "systems_per_step": NSYS,
-                                            "path": "reference CPU lu_factor + lu_solve_perm (cpu_ref_lu.c), COLAMD order from this project"},
-            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "data": "synthetic", "config": workload_config(m, world),
+            "path": "reference CPU lu_factor + lu_solve_perm (src/cpu_ref_lu.c, splu.h compiled from the "
+                    "reference's sources), one factorization per unit; column order: the GPU arm's COLAMD "
+                    "order read from oracle/power_grid_colamd_q.npy",
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": len(cores), "kind": kind,
+                             "sample": f"{args.steps} steps x {NSYS} refactor+solves, {len(cores)} worker "
+                                       f"processes pinned one per core, after {max(args.warmup, 1)} warm-up "
+                                       f"steps; median step {1000 * statistics.median(ts):.1f} ms",
+                             "cpu": host_cpu()},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -244,9 +322,12 @@ def _ev_ms(torch, fn, stream, reps, flush=None):
     return statistics.median(ts)
 
 
-def suite_uneven(torch, api, mna, oracle, stream, flush):
+def suite_uneven(torch, api, mna, oracle, stream, flush, reps=3, nsample=128):
     """512 analog matrices, n ~ U[100, 5000], distinct patterns, 8 Newton
-    refactors each: 4096 systems in one launch."""
+    refactors each: 4096 systems in one launch (one CUDA graph of the
+    engine's kernels), mixed and plain fp64 on the same inputs, L2 flushed
+    before each timed launch.  Acceptance: a seeded sample of the systems
+    against the compiled reference's fp64 solve."""
     rng = np.random.default_rng(42)
     sizes = rng.integers(100, 5001, 512)
     t0 = time.perf_counter()
@@ -262,13 +343,13 @@ def suite_uneven(torch, api, mna, oracle, stream, flush):
             owner.append(i)
     out = {"workload": "512 analog MNA matrices, n ~ U[100,5000], distinct patterns, 8 refactors each "
                        "(4096 systems per launch)", "host_analysis_s_for_512_patterns": t_an}
-    sample = np.random.default_rng(7).choice(len(vals), 128, replace=False)
+    sample = np.random.default_rng(7).choice(len(vals), nsample, replace=False)
     for prec, name in ((api.MIXED, "mixed"), (api.FP64, "fp64")):
         B = api.Batch(plist, prec=prec)
         B.upload(vals, rhs, stream=stream)
         for _ in range(2):
             B.run(api.RUN_BOTH, stream=stream, graph=True)
-        ms = _ev_ms(torch, lambda: B.run(api.RUN_BOTH, stream=stream, graph=True), stream, 3, flush)
+        ms = _ev_ms(torch, lambda: B.run(api.RUN_BOTH, stream=stream, graph=True), stream, reps, flush)
         xs = B.split(B.download(stream=stream))
         torch.cuda.synchronize()
         acc = 0
@@ -278,14 +359,18 @@ def suite_uneven(torch, api, mna, oracle, stream, flush):
             ref = oracle.ref_cpu_solve(m.n, m.Ap, m.Ai, vals[s], q, m.b)
             acc += int(np.linalg.norm(xs[s] - ref) / np.linalg.norm(ref) <= 1e-6)
         out[name] = {"ms_per_launch": ms, "systems_per_s": len(vals) / (ms / 1000.0),
-                     "accepted_in_sample": f"{acc}/{len(sample)}"}
+                     "accepted_in_sample": f"{acc}/{len(sample)}", "launches": B.launch_count()}
         B.close()
+    out["mixed_over_fp64"] = out["mixed"]["systems_per_s"] / out["fp64"]["systems_per_s"]
+    for p in pats:
+        p.close()
     return out
 
 
-def suite_large(torch, api, mna, oracle, stream, flush, lib):
+def suite_large(torch, api, mna, oracle, stream, flush, lib, spmv_reps=20, solve_reps=3):
     """n = 40,000 circuit with supply nets: SpMV variants (HBM GB/s vs the
-    measured peak) and a full mixed-precision GMRES-IR solve."""
+    measured peak, L2 flushed before each call) and a full refactor + solve
+    in both precisions, accepted against the compiled reference's solve."""
     import ctypes as C
     hbm, kind = peaks()
     m = mna.large_circuit()
@@ -304,7 +389,7 @@ def suite_large(torch, api, mna, oracle, stream, flush, lib):
     spmv = {}
 
     def rec(name, fn, sv):
-        ms = _ev_ms(torch, fn, stream, 20, flush)
+        ms = _ev_ms(torch, fn, stream, spmv_reps, flush)
         b = nnz * (sv + 4) + (n + 1) * 4 + 16 * n
         spmv[name] = {"us": ms * 1000.0, "GB_s": b / (ms / 1000.0) / 1e9, "frac": b / (ms / 1000.0) / 1e9 / hbm}
 
@@ -329,11 +414,12 @@ def suite_large(torch, api, mna, oracle, stream, flush, lib):
         B = api.Batch([P], prec=prec, inner_prec=inner, max_outer=10)
         B.upload([m.Ax], [m.b], stream=stream)
         B.run(api.RUN_BOTH, stream=stream)
-        ms = _ev_ms(torch, lambda: B.run(api.RUN_BOTH, stream=stream), stream, 3, flush)
+        ms = _ev_ms(torch, lambda: B.run(api.RUN_BOTH, stream=stream), stream, solve_reps, flush)
         xg = B.download(stream=stream)
         torch.cuda.synchronize()
         stt = B.stats(stream=stream)[0]
-        out[name] = {"refactor_solve_ms": ms, "rel_err": float(np.linalg.norm(xg - ref) / np.linalg.norm(ref)),
+        err = float(np.linalg.norm(xg - ref) / np.linalg.norm(ref))
+        out[name] = {"refactor_solve_ms": ms, "rel_err": err, "accepted": int(err <= 1e-6),
                      "status": stt["status"], "outer": stt["outer_iters"], "inner": stt["inner_iters"],
                      "dense_tail": P.info["dense_tail"]}
         B.close()
@@ -443,6 +529,70 @@ def run_suite(args):
         print(json.dumps({"suite": name, **parts[name]()}), flush=True)
 
 
+def config0(torch, api, mna, oracle, stream, flush):
+    """The analog MNA circuit n = 989 (900 nodes + 89 branch rows): the
+    reference's CPU factor+solve on one pinned core (median and best of >= 5
+    passes over 50 perturbed value sets), and the GPU paths on the same value
+    sets: one request at a time (p50 device time) and the 50 as one batch."""
+    m = mna.analog(989, 42)
+    vals = m.perturbed(NSYS, seed=989)
+    P = api.Pattern.from_matrix(m)
+    _, q = P.perm()
+    units = [(m.n, m.Ap, m.Ai, v, q, m.b) for v in vals]
+    ts, core, kind = cpu_pinned_pass_times(units, repeats=7)
+    refs = [oracle.ref_cpu_solve(*u) for u in units]
+    out = {"workload": f"analog MNA n={m.n}, nnz={m.nnz} (900 nodes + 89 branch rows), {NSYS} value sets",
+           "cpu_reference_1core": {"kind": kind, "core": core, "passes": len(ts),
+                                   "factor_solve_ms_median": 1000 * statistics.median(ts) / len(units),
+                                   "factor_solve_ms_best": 1000 * min(ts) / len(units)}}
+    for prec, name in ((api.MIXED, "mixed"), (api.FP64, "fp64")):
+        b1 = api.Batch([P], prec=prec)
+        times, acc = [], 0
+        for s_ in range(NSYS):
+            b1.upload([vals[s_]], [m.b], stream=stream)
+            a, bq = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            b1.run(api.RUN_BOTH, stream=stream)
+            bq.record(stream)
+            x = b1.download(stream=stream)
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(bq))
+            acc += int(np.linalg.norm(x - refs[s_]) / np.linalg.norm(refs[s_]) <= 1e-6)
+        b1.close()
+        B = api.Batch([P] * NSYS, prec=prec)
+        B.upload(list(vals), np.tile(m.b, NSYS), stream=stream)
+        for _ in range(3):
+            B.run(api.RUN_BOTH, stream=stream, graph=True)
+        ms = _ev_ms(torch, lambda: B.run(api.RUN_BOTH, stream=stream, graph=True), stream, 5, flush)
+        xs = B.split(B.download(stream=stream))
+        torch.cuda.synchronize()
+        accb = sum(int(np.linalg.norm(xs[i] - refs[i]) / np.linalg.norm(refs[i]) <= 1e-6) for i in range(NSYS))
+        B.close()
+        out[name] = {"single_request_p50_ms": float(np.percentile(times, 50)),
+                     "single_request_accepted": f"{acc}/{NSYS}",
+                     "batched_ms_per_launch": ms, "batched_systems_per_s": NSYS / (ms / 1000.0),
+                     "batched_accepted": f"{accb}/{NSYS}"}
+    P.close()
+    return out
+
+
+def timed_steps(torch, fn, stream, steps, flush):
+    """Per-step device times (ms) of fn() on stream: before each step a short
+    device-side spin (the host queues the step before the GPU reaches it) and
+    an L2 flush (256 MiB write), then CUDA events around the step."""
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        with torch.cuda.stream(stream):
+            torch.cuda._sleep(HOST_AHEAD_CYCLES)
+            flush.fill_(float(i))
+            ev[i][0].record(stream)
+        fn()
+        with torch.cuda.stream(stream):
+            ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -450,6 +600,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other workloads' keys (configs 0, 2, 3) of the default line")
     ap.add_argument("--suite", default="", help="comma list of uneven,large,serving: the other "
                     "workloads, one JSON line each, instead of the default run")
     args = ap.parse_args()
@@ -473,46 +625,49 @@ def main():
     rhs = np.tile(m.b, NSYS)
     B = api.Batch([P] * NSYS, prec=api.MIXED, krylov=30)
     B.upload(list(vals), rhs, stream=stream)
+    B64 = api.Batch([P] * NSYS, prec=api.FP64)
+    B64.upload(list(vals), rhs, stream=stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def step(batch, what=api.RUN_BOTH):
         batch.run(what, stream=stream, graph=True)
 
-    # Warm-up (captures the graph), then timed steps with an L2 flush between.
+    # Warm-up (captures the graphs), then timed steps, L2 flushed between.
     for _ in range(max(args.warmup, 3)):
         step(B)
+        step(B64)
     torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         t0 = time.perf_counter()
-        for i in range(args.steps):
-            with torch.cuda.stream(stream):
-                torch.cuda._sleep(HOST_AHEAD_CYCLES)
-                flush.fill_(float(i))
-                ev[i][0].record(stream)
-            step(B)
-            with torch.cuda.stream(stream):
-                ev[i][1].record(stream)
-        torch.cuda.synchronize()
+        kern_ms = timed_steps(torch, lambda: step(B), stream, args.steps, flush)
         wall = time.perf_counter() - t0
     barrier(world)
-    kern_ms = [a.elapsed_time(b) for a, b in ev]
     step_ms = max_over_ranks(statistics.mean(kern_ms), world)
+    # The plain fp64 GPU path on the same inputs, same protocol (spin, flush,
+    # per-step events, mean over the same number of steps).
+    k64 = timed_steps(torch, lambda: step(B64), stream, args.steps, flush)
+    fp64_ms = max_over_ranks(statistics.mean(k64), world)
 
-    # Accuracy gate against the fp64 oracle (same value sets).
+    # Accuracy gate against the fp64 oracle (same value sets, same column
+    # order): the compiled reference's lu_factor + lu_solve_perm.
     from oracle import oracle
+    refs = [oracle.ref_cpu_solve(m.n, m.Ap, m.Ai, vals[s], q, m.b) for s in range(NSYS)]
+
+    def accept(xs):
+        errs = [float(np.linalg.norm(xs[s] - refs[s]) / np.linalg.norm(refs[s])) for s in range(NSYS)]
+        return sum(int(e <= 1e-6) for e in errs), errs
+
     xs = B.split(B.download(stream=stream))
     torch.cuda.synchronize()
     stats = B.stats(stream=stream)
-    accepted, errs = 0, []
-    for s in range(NSYS):
-        ref = oracle.ref_cpu_solve(m.n, m.Ap, m.Ai, vals[s], q, m.b)
-        e = float(np.linalg.norm(xs[s] - ref) / np.linalg.norm(ref))
-        errs.append(e)
-        accepted += int(e <= 1e-6)
+    accepted, errs = accept(xs)
+    x64 = B64.split(B64.download(stream=stream))
+    torch.cuda.synchronize()
+    acc64, errs64 = accept(x64)
     value = accepted * world / (step_ms / 1000.0)
+    value64 = acc64 * world / (fp64_ms / 1000.0)
 
     # Roofline of the dominant kernel: the sparse refactor kernel (the largest
     # share of GPU time in the ncu launch list of this program), with the
@@ -521,19 +676,23 @@ def main():
     # (lusp_batch_time_kernels), L2 flushed before each timed launch.
     hbm, peak_kind = peaks()
     alg_ref, alg = algorithmic_bytes(info, stats, vs=4)
-    B.time_kernels(True)
-    kms = []
-    for i in range(max(3, args.steps // 2)):
-        with torch.cuda.stream(stream):
-            torch.cuda._sleep(HOST_AHEAD_CYCLES)
-            flush.fill_(float(i))
-        B.run(api.RUN_BOTH, stream=stream)
-        kms.append(B.kernel_ms())
-    torch.cuda.synchronize()
-    B.time_kernels(False)
-    refactor_ms = statistics.mean(k["refactor"] for k in kms)
-    dense_ms = statistics.mean(k["dense"] for k in kms)
-    solve_ms = statistics.mean(k["solve"] for k in kms)
+
+    def kernel_times(batch):
+        batch.time_kernels(True)
+        kms = []
+        for i in range(max(3, args.steps // 2)):
+            with torch.cuda.stream(stream):
+                torch.cuda._sleep(HOST_AHEAD_CYCLES)
+                flush.fill_(float(i))
+            batch.run(api.RUN_BOTH, stream=stream)
+            kms.append(batch.kernel_ms())
+        torch.cuda.synchronize()
+        batch.time_kernels(False)
+        return {k: statistics.mean(d[k] for d in kms) for k in ("refactor", "dense", "solve")}
+
+    kt = kernel_times(B)
+    kt64 = kernel_times(B64)
+    refactor_ms, dense_ms, solve_ms = kt["refactor"], kt["dense"], kt["solve"]
     achieved_ref = alg_ref / (refactor_ms / 1000.0) / 1e9
     achieved = alg / (solve_ms / 1000.0) / 1e9
 
@@ -541,26 +700,8 @@ def main():
         prof = ROOT / "profiles" / name
         return json.loads(prof.read_text()).get("dram_bytes_per_launch") if prof.exists() else None
 
-    # Plain fp64 GPU path on the same inputs: batched, and per request.
-    B64 = api.Batch([P] * NSYS, prec=api.FP64)
-    B64.upload(list(vals), rhs, stream=stream)
-    for _ in range(3):
-        step(B64)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    reps = max(3, args.steps // 2)
-    for _ in range(reps):
-        step(B64)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    fp64_batched_ms = e0.elapsed_time(e1) / reps
-    x64 = B64.split(B64.download(stream=stream))
-    torch.cuda.synchronize()
-    acc64 = sum(int(np.linalg.norm(x64[s] - oracle.ref_cpu_solve(m.n, m.Ap, m.Ai, vals[s], q, m.b)) /
-                    np.linalg.norm(x64[s]) <= 1e-6) for s in range(NSYS))
-    single = {}
-    lat = {}
+    # Single requests (one system per launch, no graph): latency p50 / p99.
+    single, lat = {}, {}
     for prec in (api.FP64, api.MIXED):
         b1 = api.Batch([P], prec=prec)
         times = []
@@ -575,7 +716,6 @@ def main():
         single[prec] = statistics.mean(times)
         lat[prec] = (float(np.percentile(times, 50)), float(np.percentile(times, 99)))
         b1.close()
-    fp64_per_request_rate = 1000.0 / single[api.FP64]
 
     # End to end through the public API with pinned host buffers: every step
     # copies its values and right-hand sides host->device, runs the graph and
@@ -644,29 +784,40 @@ def main():
     d2h = int(x_nps[0].nbytes)
     # The end-to-end results are the device-timed step's results.
     e2e_same = all(bool(np.array_equal(x, np.concatenate(xs))) for x in x_nps)
+    launches = args.steps * B.launch_count()
+    B.close()
+    B2.close()
+    B64.close()
 
     line = None
     if rank == 0:
-        cpu = None
-        if not args.no_cpu:
-            rate, sample, kind = cpu_reference_rate(m, vals, q, 1, budget_s=10.0)
-            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample}
+        cpu = None if args.no_cpu else cpu_baseline_1core(m, vals, q)
+        extra = {}
+        if world == 1 and not args.no_configs:
+            from luspice_b200 import _lib
+            extra["config0_analog_989"] = config0(torch, api, mna, oracle, stream, flush)
+            extra["config2_uneven_512x8"] = suite_uneven(torch, api, mna, oracle, stream, flush, reps=3,
+                                                         nsample=64)
+            extra["config3_large_40k"] = suite_large(torch, api, mna, oracle, stream, flush, _lib.load(),
+                                                     spmv_reps=10, solve_reps=2)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "systems_per_step": NSYS, "n": m.n, "nnz": m.nnz,
-                       "lu_slots": info["cap"], "col_levels": info["ncol_levels"],
-                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                       "graph": True},
+            "config": workload_config(m, world),
+            "setup": {"method": METHOD, "lu_slots": info["cap"], "col_levels": info["ncol_levels"], "dense_tail": info["dense_tail"],
+                      "l2": "flushed between timed steps (256 MiB write)", "graph": True},
             "accepted": accepted, "max_rel_err": max(errs),
             "mean_inner_iters": float(np.mean([s["inner_iters"] for s in stats])),
             "latency_ms": {"mixed_p50": lat[api.MIXED][0], "mixed_p99": lat[api.MIXED][1],
                            "fp64_p50": lat[api.FP64][0], "fp64_p99": lat[api.FP64][1]},
-            "fp64_gpu": {"per_request_rate": fp64_per_request_rate, "batched_rate": NSYS * 1000.0 / fp64_batched_ms,
-                         "batched_accepted": acc64,
-                         "mixed_batched_over_fp64_per_request": value / world / fp64_per_request_rate,
-                         "mixed_batched_over_fp64_batched": (NSYS * 1000.0 / step_ms) / (NSYS * 1000.0 / fp64_batched_ms)},
+            "fp64_gpu": {"batched_rate": value64, "batched_ms_per_step": fp64_ms,
+                         "batched_accepted": acc64, "batched_max_rel_err": max(errs64),
+                         "per_request_rate": 1000.0 / single[api.FP64],
+                         "protocol": "same as value: spin + L2 flush before each step, CUDA events per step, "
+                                     "mean of the same number of steps",
+                         "kernel_ms": kt64,
+                         "mixed_over_fp64_batched": value / value64 if value64 > 0 else None},
             "e2e": {"value": accepted * world / (serial_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": serial_ms,
                     "pipelining": "none: each step's copies, graph and read-back in order on one stream",
@@ -684,15 +835,14 @@ def main():
                          "solve_kernel": {"achieved": achieved, "frac": achieved / hbm,
                                           "traffic": traffic_of("solve_kernel_power_grid4050x50.json"),
                                           "alg_bytes_per_launch": alg, "kernel_ms": solve_ms}},
-            "gpu_launches": args.steps * B.launch_count(),
+            "gpu_launches": launches,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "wall_s_timed": wall,
+            **extra,
         }
         print(json.dumps(line), flush=True)
-    B.close()
-    B2.close()
-    B64.close()
+    P.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

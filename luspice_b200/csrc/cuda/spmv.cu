@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256)
 sell_kernel(int nslices, const int* __restrict__ ptr, const int* __restrict__ col,
             const VT* __restrict__ val, const int* __restrict__ perm,
             const double* __restrict__ x, double* __restrict__ y,
-            const double* __restrict__ row_scale, int sell_blocks, int nlong,
+            const double* __restrict__ row_div, int sell_blocks, int nlong,
             const int* __restrict__ lrow, const int* __restrict__ lptr, const int* __restrict__ lcol,
             const VT* __restrict__ lval) {
     if ((int)blockIdx.x >= sell_blocks) {
@@ -95,7 +95,7 @@ sell_kernel(int nslices, const int* __restrict__ ptr, const int* __restrict__ co
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) {
             const int row = lrow[w];
-            y[row] = row_scale ? acc * row_scale[row] : acc;
+            y[row] = row_div ? acc / row_div[row] : acc;
         }
         return;
     }
@@ -125,14 +125,15 @@ sell_kernel(int nslices, const int* __restrict__ ptr, const int* __restrict__ co
     for (int o = 16; o >= C; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (sub == 0) {
         const int row = perm[s * C + r];
-        if (row >= 0) y[row] = row_scale ? acc * row_scale[row] : acc;
+        if (row >= 0) y[row] = row_div ? acc / row_div[row] : acc;
     }
 }
 
-__global__ void scale_kernel(int n, const double* __restrict__ x, const double* __restrict__ s,
-                             double* __restrict__ out) {
+// out = x / s elementwise (the column scaling undone on the input vector).
+__global__ void unscale_kernel(int n, const double* __restrict__ x, const double* __restrict__ s,
+                               double* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = x[i] * s[i];
+    if (i < n) out[i] = x[i] / s[i];
 }
 
 }  // namespace
@@ -144,7 +145,7 @@ struct SellObj {
     int* d_col = nullptr;
     void* d_val = nullptr;
     int* d_perm = nullptr;
-    double* d_rinv = nullptr;   // fp16: 1 / row scale
+    double* d_rs = nullptr;     // fp16: row scale
     double* d_cs = nullptr;     // fp16: column scale
     double* d_xs = nullptr;     // fp16: scaled x
     double smin = 0, smax = 0;
@@ -398,12 +399,10 @@ int lusp_sell_create(int n, const int* rowptr, const int* colidx, const double* 
             }
         }
         if (e == cudaSuccess && value_kind == 2) {
-            std::vector<double> rinv(n);
-            for (int i = 0; i < n; i++) rinv[i] = 1.0 / rs[i];
-            e = cudaMalloc((void**)&S->d_rinv, n * sizeof(double));
+            e = cudaMalloc((void**)&S->d_rs, n * sizeof(double));
             if (e == cudaSuccess) e = cudaMalloc((void**)&S->d_cs, n * sizeof(double));
             if (e == cudaSuccess) e = cudaMalloc((void**)&S->d_xs, n * sizeof(double));
-            if (e == cudaSuccess) e = cudaMemcpy(S->d_rinv, rinv.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpy(S->d_rs, rs.data(), n * sizeof(double), cudaMemcpyHostToDevice);
             if (e == cudaSuccess) e = cudaMemcpy(S->d_cs, cs.data(), n * sizeof(double), cudaMemcpyHostToDevice);
         }
         if (e != cudaSuccess) {
@@ -425,7 +424,7 @@ void lusp_sell_destroy(lusp_sell* hs) {
     cudaFree(S->d_col);
     cudaFree(S->d_val);
     cudaFree(S->d_perm);
-    cudaFree(S->d_rinv);
+    cudaFree(S->d_rs);
     cudaFree(S->d_cs);
     cudaFree(S->d_xs);
     cudaFree(S->d_lrow);
@@ -441,13 +440,14 @@ int lusp_sell_spmv(const lusp_sell* hs, const double* d_x, double* d_y, void* st
     cudaStream_t st = (cudaStream_t)stream;
     const double* xin = d_x;
     if (S->kind == 2) {
-        scale_kernel<<<(S->n + 255) / 256, 256, 0, st>>>(S->n, d_x, S->d_cs, S->d_xs);
+        // A x = Dr^-1 (Dr A Dc) (Dc^-1 x): the stored values are Dr A Dc.
+        unscale_kernel<<<(S->n + 255) / 256, 256, 0, st>>>(S->n, d_x, S->d_cs, S->d_xs);
         xin = S->d_xs;
     }
     const int sell_blocks = (int)(((long)S->nslices * 32 + 255) / 256);
     const int long_blocks = (int)(((long)S->nlong * 32 + 255) / 256);
     const int grid = sell_blocks + long_blocks;
-    const double* rsc = S->kind == 2 ? S->d_rinv : nullptr;
+    const double* rsc = S->kind == 2 ? S->d_rs : nullptr;
 #define LUSP_SELL_CASE(CC)                                                                        \
     if (S->C == CC) {                                                                             \
         if (S->kind == 0)                                                                         \

@@ -9,7 +9,9 @@ this module.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -26,11 +28,24 @@ _orc = None
 _ref = None
 
 
-def build(ref_root: str | None = "/root/reference") -> None:
-    """Build liboracle.so, and _ref/ when the reference tree is present."""
+REF_ENV = "LUSPICE_REF_ROOT"
+
+
+def build(ref_root: str | None = None) -> None:
+    """Build liboracle.so, and _ref/ from the reference's sources.
+
+    ref_root: the LUSpice source tree (default: the LUSPICE_REF_ROOT
+    environment variable).  Without either, only the restatement is built and
+    a message says why _ref/ was not (an existing _ref/ is kept)."""
     subprocess.run(["make", "-s", "oracle"], cwd=HERE, check=True)
-    if ref_root and Path(ref_root).is_dir():
-        subprocess.run(["make", "-s", "ref", f"REF={ref_root}"], cwd=HERE, check=True)
+    root = ref_root or os.environ.get(REF_ENV)
+    if not root:
+        print(f"oracle: {REF_ENV} is not set and no reference tree was given: "
+              f"_ref/ (the reference compiled from its sources) not rebuilt", file=sys.stderr)
+        return
+    if not (Path(root) / "src" / "third_party" / "splu.h").is_file():
+        raise FileNotFoundError(f"oracle: {root} is not a LUSpice source tree (no src/third_party/splu.h)")
+    subprocess.run(["make", "-s", "ref", f"REF={root}"], cwd=HERE, check=True)
 
 
 def _p(a, t):
@@ -160,22 +175,27 @@ def lu_solve(F, q, b, use_ref_handle=None):
 
 
 def ref_cpu_solve(n, Ap, Ai, Ax, q, b, tol=1.0):
-    """The reference's CPU path: lu_factor + lu_solve_perm (cpu_ref_lu.c
-    restated with a modest initial capacity).  Returns x or None if singular."""
-    F = lu_factor(n, Ap, Ai, Ax, q, tol)
+    """The reference's CPU path (src/cpu_ref_lu.c:15-58): one lu_factor, then
+    lu_solve_perm with the same factors, with a modest initial capacity
+    instead of cpu_ref_lu.c's n*n slots.  The compiled reference when it is
+    built, else the restatement.  Returns x, or None if singular."""
+    Ap, Ai, Ax, bb = _i32(Ap), _i32(Ai), _f64(Ax), _f64(b)
+    qq = None if q is None else _i32(q)
+    if ref_available():
+        lib = ref()
+        h = lib.ref_lu_factor(n, _p(Ap, C.c_int), _p(Ai, C.c_int), _p(Ax, C.c_double), _p(qq, C.c_int), tol)
+        try:
+            if lib.ref_lu_status(h) >= 0:
+                return None
+            x = np.empty(n)
+            lib.ref_lu_solve(h, _p(qq, C.c_int), _p(bb, C.c_double), _p(x, C.c_double))
+            return x
+        finally:
+            lib.ref_lu_free(h)
+    F = lu_factor(n, Ap, Ai, Ax, q, tol, use_ref=False)
     if F["status"] >= 0:
         return None
-    if ref_available():
-        Ap, Ai, Ax = _i32(Ap), _i32(Ai), _f64(Ax)
-        lib = ref()
-        qq = None if q is None else _i32(q)
-        h = lib.ref_lu_factor(n, _p(Ap, C.c_int), _p(Ai, C.c_int), _p(Ax, C.c_double), _p(qq, C.c_int), tol)
-        x = np.empty(n)
-        bb = _f64(b)
-        lib.ref_lu_solve(h, _p(qq, C.c_int), _p(bb, C.c_double), _p(x, C.c_double))
-        lib.ref_lu_free(h)
-        return x
-    return lu_solve(F, q, b)
+    return lu_solve(F, q, bb)
 
 
 def dense_factor(n, Ap, Ai, Ax, diagrow):

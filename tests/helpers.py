@@ -56,5 +56,45 @@ def rel_res(m, values, x, b):
     return float(np.linalg.norm(m.matvec(x, values) - b) / max(np.linalg.norm(b), 1e-300))
 
 
+FP16_MIN_NORMAL = 2.0 ** -14
+
+
+def ruiz_scaling(n, Ap, Ai, values, sweeps=30, tol=1e-6):
+    """Restatement of the Ruiz equilibration both the standalone SELL
+    (lusp_ruiz_csr) and the engine's fp16 inner products run: row maxima of
+    |a| r_i c_j, r_i /= sqrt(max), then column maxima, c_j /= sqrt(max),
+    until every maximum is within tol of 1 (at most `sweeps` sweeps).  The
+    maxima do not depend on the order entries are visited in, so CSC input
+    gives the same r, c as the CSR loops.  Returns (r, c, rows, cols)."""
+    cols = np.repeat(np.arange(n), np.diff(Ap))
+    rows = np.asarray(Ai, dtype=np.int64)
+    a = np.abs(values)
+    r = np.ones(n)
+    c = np.ones(n)
+    for _ in range(sweeps):
+        dev = 0.0
+        rm = np.zeros(n)
+        np.maximum.at(rm, rows, a * r[rows] * c[cols])
+        nz = rm > 0
+        r[nz] = r[nz] / np.sqrt(rm[nz])
+        dev = max(dev, float(np.max(np.abs(1.0 - rm[nz]), initial=0.0)))
+        cm = np.zeros(n)
+        np.maximum.at(cm, cols, a * r[rows] * c[cols])
+        nz = cm > 0
+        c[nz] = c[nz] / np.sqrt(cm[nz])
+        dev = max(dev, float(np.max(np.abs(1.0 - cm[nz]), initial=0.0)))
+        if dev < tol:
+            break
+    return r, c, rows, cols
+
+
+def ruiz_fits_fp16(m, values):
+    """Whether every Ruiz-scaled nonzero lies in the fp16 normal range."""
+    r, c, rows, cols = ruiz_scaling(m.n, m.Ap, m.Ai, values)
+    s = np.abs(values * r[rows] * c[cols])
+    s = s[s != 0]
+    return bool(s.min() >= FP16_MIN_NORMAL and s.max() <= 65504.0)
+
+
 def small_problems():
     return [mna.analog(120, 7), mna.analog(989, 42), mna.power_grid(15, 16, 6, seed=3)]

@@ -269,3 +269,36 @@ def test_library_fails_loudly_without_build(tmp_path, monkeypatch):
         L.load(tmp_path / "nope.so")
     monkeypatch.setattr(L, "_lib", None)
     importlib.reload(L)
+
+
+def test_reference_arm_column_order_fixture():
+    """bench.py's reference arm reads the power grid's column order from a
+    committed file (that process never loads the product library); the file
+    is the library's COLAMD order of the same matrix."""
+    q = np.load(ROOT / "oracle" / "power_grid_colamd_q.npy")
+    m = mna.power_grid()
+    assert np.array_equal(q, api.colamd(m.n, m.Ap, m.Ai))
+
+
+def test_cpu_reference_solve_factors_once(monkeypatch):
+    """ref_cpu_solve runs one factorization per solve (the timed CPU unit is
+    one factor + one solve) and matches the restatement's answer."""
+    if not O.ref_available():
+        pytest.skip("compiled reference (oracle/_ref) not built")
+    m = mna.analog(300, 3)
+    q = api.colamd(m.n, m.Ap, m.Ai)
+    lib = O.ref()
+    calls = []
+    real = lib.ref_lu_factor
+
+    class Counting:
+        def __call__(self, *a):
+            calls.append(1)
+            return real(*a)
+
+    monkeypatch.setattr(lib, "ref_lu_factor", Counting())
+    x = O.ref_cpu_solve(m.n, m.Ap, m.Ai, m.Ax, q, m.b)
+    assert len(calls) == 1
+    monkeypatch.undo()
+    F = O.lu_factor(m.n, m.Ap, m.Ai, m.Ax, q, use_ref=False)
+    assert np.array_equal(x.view(np.uint64), O.lu_solve(F, q, m.b).view(np.uint64))

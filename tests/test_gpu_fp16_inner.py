@@ -5,42 +5,9 @@ import numpy as np
 import pytest
 
 from luspice_b200 import api, mna
-from tests.helpers import TOL_REL, oracle_solution, rel_err, rel_res
+from tests.helpers import TOL_REL, oracle_solution, rel_err, rel_res, ruiz_fits_fp16
 
 pytestmark = pytest.mark.gpu
-
-FP16_MIN_NORMAL = 2.0 ** -14
-
-
-def ruiz_fits_fp16(m, values, sweeps=30, tol=1e-6):
-    """Restatement of the equilibration the device runs (row maxima of
-    |a| r_i c_j, r_i /= sqrt(max), then column maxima, c_j /= sqrt(max),
-    until every maximum is within tol of 1), and the range test of the
-    scaled nonzeros against the fp16 normal range."""
-    n = m.n
-    cols = np.repeat(np.arange(n), np.diff(m.Ap))
-    rows = m.Ai.astype(np.int64)
-    a = np.abs(values)
-    r = np.ones(n)
-    c = np.ones(n)
-    for _ in range(sweeps):
-        dev = 0.0
-        rm = np.zeros(n)
-        np.maximum.at(rm, rows, a * r[rows] * c[cols])
-        nz = rm > 0
-        r[nz] = r[nz] / np.sqrt(rm[nz])
-        dev = max(dev, float(np.max(np.abs(1.0 - rm[nz]), initial=0.0)))
-        cm = np.zeros(n)
-        np.maximum.at(cm, cols, a * r[rows] * c[cols])
-        nz = cm > 0
-        c[nz] = c[nz] / np.sqrt(cm[nz])
-        dev = max(dev, float(np.max(np.abs(1.0 - cm[nz]), initial=0.0)))
-        if dev < tol:
-            break
-    s = np.abs(values * r[rows] * c[cols])
-    s = s[s != 0]
-    return bool(s.min() >= FP16_MIN_NORMAL and s.max() <= 65504.0)
-
 
 @pytest.mark.parametrize("case", ["grid", "analog"])
 def test_fp16_inner_products_where_they_fit(gpu, case):

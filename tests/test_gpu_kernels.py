@@ -8,6 +8,7 @@ import scipy.sparse as sp
 
 from luspice_b200 import api, mna
 from oracle import oracle as O
+from tests.helpers import FP16_MIN_NORMAL, ruiz_scaling
 
 pytestmark = pytest.mark.gpu
 
@@ -112,20 +113,50 @@ def test_sell_spmv(gpu, Cc, sigma, kind):
 
 
 def test_sell_fp16_ruiz(gpu):
+    """fp16 SELL values on the n = 4050 power grid, whose Ruiz-scaled range
+    fits the fp16 normal range: sell_kernel<C, __half> against a host SpMV
+    on the same fp16-rounded scaled values (only the summation order
+    differs), and against the exact product within the fp16 storage bound
+    (each stored value within 2^-11 of the scaled entry)."""
     import torch
+    m = mna.power_grid()
+    A = m.csr()
+    n = m.n
+    rows = np.repeat(np.arange(n), np.diff(A.indptr))
+    assert A.nnz == m.nnz                      # no duplicate entries: same entries as the CSC
+    r, c, _, _ = ruiz_scaling(n, m.Ap, m.Ai, m.Ax)
+    scaled = A.data * r[rows] * c[A.indices]
+    assert np.abs(scaled).min() >= FP16_MIN_NORMAL and np.abs(scaled).max() <= 65504.0
+    h = scaled.astype(np.float16).astype(np.float64)
+    for Cc in (32, 16, 8):
+        S = api.Sell(n, A.indptr, A.indices, A.data, Cc, 256, "fp16")
+        for seed in (2, 3):
+            x = np.random.default_rng(seed).standard_normal(n)
+            dx = _dev(torch, x, torch.float64)
+            dy = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
+            S.spmv(dx.data_ptr(), dy.data_ptr())
+            torch.cuda.synchronize()
+            y = dy.cpu().numpy()
+            xs = x / c
+            ref16 = (sp.csr_matrix((h, A.indices, A.indptr), shape=A.shape) @ xs) / r
+            mag16 = (sp.csr_matrix((np.abs(h), A.indices, A.indptr), shape=A.shape) @ np.abs(xs)) / r
+            assert np.all(np.abs(y - ref16) <= 1e-13 * mag16 + 1e-300), (Cc, seed)
+            exact = A @ x
+            assert np.all(np.abs(y - exact) <= 2.0 ** -10 * (np.abs(A) @ np.abs(x)) + 1e-300), (Cc, seed)
+            assert np.linalg.norm(y - exact) / np.linalg.norm(exact) <= 1e-3
+        S.close()
+
+
+def test_sell_fp16_refused_outside_fp16_range(gpu):
+    """An analog circuit (gmin 1e-12 beside 1e-1 conductances): the scaled
+    values cannot all be fp16 normals, so the fp16 SELL is refused."""
     m = mna.analog(1500, 4)
     A = m.csr()
-    try:
-        S = api.Sell(m.n, A.indptr, A.indices, A.data, 32, 256, "fp16")
-    except api.LuspError:
-        pytest.skip("scaled range outside fp16 normal range for this matrix")
-    x = np.random.default_rng(2).standard_normal(m.n)
-    dx, dy = _dev(torch, x, torch.float64), torch.zeros(m.n, dtype=torch.float64, device="cuda")
-    S.spmv(dx.data_ptr(), dy.data_ptr())
-    torch.cuda.synchronize()
-    ref = A @ x
-    # fp16 storage: relative error of each product <= 2^-11.
-    assert np.all(np.abs(dy.cpu().numpy() - ref) <= 2.0 ** -10 * (np.abs(A) @ np.abs(x)) + 1e-300)
+    r, c, rows, cols = ruiz_scaling(m.n, m.Ap, m.Ai, m.Ax)
+    s = np.abs(m.Ax * r[rows] * c[cols])
+    assert s[s != 0].min() < FP16_MIN_NORMAL
+    with pytest.raises(api.LuspError, match="fp16 normal range"):
+        api.Sell(m.n, A.indptr, A.indices, A.data, 32, 256, "fp16")
 
 
 def test_csr_spmv32(gpu, lib):

@@ -65,6 +65,39 @@ def test_noalloc_trisolve_matches_regular_entry_point(gpu, lib):
         assert np.array_equal(c.view(np.uint64), xh.view(np.uint64))
 
 
+def test_noalloc_trisolve_without_column_order(gpu, lib):
+    """q = NULL (x returned in pivot-column order, as lu_solve_perm with no
+    column permutation): the same bits as the regular entry point given
+    q = NULL, on two calls in a row."""
+    import torch
+    m = mna.analog(600, 11)
+    q = api.colamd(m.n, m.Ap, m.Ai)
+    F = O.lu_factor(m.n, m.Ap, m.Ai, m.Ax, q)
+    assert F["status"] == -1
+    n = m.n
+    t = {k: _dev(torch, F[k], torch.int32) for k in ("Lp", "Li", "Up", "Ui", "pinv")}
+    t.update({k: _dev(torch, F[k], torch.float64) for k in ("Lx", "Ux")})
+    wi = torch.zeros(n, dtype=torch.int32, device="cuda")
+    wd = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+    rng = np.random.default_rng(9)
+    for call in range(2):
+        b = _dev(torch, rng.standard_normal(n), torch.float64)
+        x_ref = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
+        x_new = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
+        assert lib.lusp_trisolve_par_launch(n, _p(t["Lp"]), _p(t["Li"]), _p(t["Lx"]), _p(t["Up"]), _p(t["Ui"]),
+                                            _p(t["Ux"]), _p(t["pinv"]), None, _p(b), _p(x_ref), _p(wi), _p(wd),
+                                            None) == 0
+        rc = lib.lusp_trisolve_par_noalloc(n, _p(t["Lp"]), _p(t["Li"]), _p(t["Lx"]), _p(t["Up"]), _p(t["Ui"]),
+                                           _p(t["Ux"]), _p(t["pinv"]), None, _p(b), _p(x_new), None)
+        assert rc == 0, lib.lusp_last_error()
+        torch.cuda.synchronize()
+        a, c = x_ref.cpu().numpy(), x_new.cpu().numpy()
+        assert np.all(np.isfinite(c))
+        assert np.array_equal(a.view(np.uint64), c.view(np.uint64)), f"call {call}"
+        xh = O.lu_solve(F, None, b.cpu().numpy())
+        assert np.array_equal(c.view(np.uint64), xh.view(np.uint64))
+
+
 def test_noalloc_trisolve_rejects_oversize(gpu, lib):
     import torch
     dummy = torch.zeros(4, dtype=torch.int32, device="cuda")
