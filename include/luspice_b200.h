@@ -215,12 +215,17 @@ int lusp_batch_run_graph(lusp_batch *b, int what, void *stream);
 /* Copy per-system statistics to the host (synchronizes the stream). */
 int lusp_batch_stats(lusp_batch *b, lusp_sys_stats *out, void *stream);
 /* Merged factor values of one system (cap entries; float for LUSP_MIXED,
- * double for LUSP_FP64), synchronizing copy. */
+ * double for LUSP_FP64), synchronizing copy.  The engine's refactor keeps
+ * only the strict-L part current in this layout (the solves read U, the
+ * diagonal and the dense trailing block from their own arrays); this call
+ * completes the array on `stream` before copying it. */
 int lusp_batch_factor_values(lusp_batch *b, int sys, void *out, void *stream);
 /* Device-to-device copy of all input values from src to dst (both batches
  * must hold the same patterns in the same order). */
 int lusp_batch_copy_values(lusp_batch *dst, const lusp_batch *src, void *stream);
-/* Device pointer to the merged factor values of one system. */
+/* Device pointer to the merged factor values of one system, completed
+ * (as lusp_batch_factor_values does) by a kernel on the default stream;
+ * later runs leave only the strict-L part current until the next call. */
 int lusp_batch_factor_device_ptr(lusp_batch *b, int sys, void **d_values);
 /* Update max_outer, rtol, inner_rel, stag_ratio, pivot_tol, xtol,
  * factor_shift and hard_shift, for the ladder's rungs too (prec, krylov,

@@ -272,6 +272,8 @@ int lusp_batch_factor_values(lusp_batch* hb, int sys, void* out, void* stream) {
     if (!B || !out || sys < 0 || sys >= B->nsys) return LUSP_EARG;
     const size_t vs = B->prec == LUSP_FP64 ? 8 : 4;
     cudaStream_t st = (cudaStream_t)stream;
+    int rc = lusp::batch_merge_factor(B, sys, st);
+    if (rc != LUSP_OK) return rc;
     cudaError_t e = cudaMemcpyAsync(out, B->h_sys[sys].lu, B->pats[sys]->S.cap * vs, cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return lusp::cuda_fail(e, "factor copy");
     e = cudaStreamSynchronize(st);
@@ -293,6 +295,10 @@ int lusp_batch_copy_values(lusp_batch* hd, const lusp_batch* hs, void* stream) {
 int lusp_batch_factor_device_ptr(lusp_batch* hb, int sys, void** d_values) {
     BatchObj* B = BO(hb);
     if (!B || !d_values || sys < 0 || sys >= B->nsys) return LUSP_EARG;
+    // Complete the merged array (default stream: ordered after the caller's
+    // earlier runs on it, and before its later work).
+    int rc = lusp::batch_merge_factor(B, sys, nullptr);
+    if (rc != LUSP_OK) return rc;
     *d_values = B->h_sys[sys].lu;
     return LUSP_OK;
 }

@@ -175,6 +175,40 @@ solve_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan
     }
 }
 
+// The merged slot array of one system, completed for callers that read the
+// factor in that layout: the engine's refactor stores the strict-L part
+// there (the later columns' gathers read it) and the U part, the diagonal
+// and the dense trailing block only in the arrays the solves read.  A CTA
+// per column (grid-stride).
+template <typename VT>
+__global__ void merge_factor_kernel(SysDev S) {
+    const PatternDev& P = *S.pat;
+    const int n = P.n, k0 = P.k0, ld = P.tail_ld;
+    VT* lu = (VT*)S.lu;
+    const VT* uval = (const VT*)S.uval;
+    const VT* udiag = (const VT*)S.udiag;
+    const VT* T = (const VT*)S.tail;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int c0 = P.cp[k], c1 = P.cp[k + 1], d = P.dg[k];
+        for (int p = c0 + (int)threadIdx.x; p < c1; p += blockDim.x) {
+            const int r = P.ri[p];
+            if (k >= k0 && r >= k0) lu[p] = T[(size_t)(k - k0) * ld + (r - k0)];
+            else if (p < d) lu[p] = uval[P.slot_dst[p]];
+            else if (p == d) lu[p] = udiag[k];
+        }
+    }
+}
+
+int batch_merge_factor(BatchObj* B, int sys, cudaStream_t st) {
+    const SysDev& S = B->h_sys[sys];
+    const int n = B->pats[sys]->S.n;
+    const int grid = std::max(1, std::min(n, 4 * sm_count()));
+    if (B->prec == LUSP_FP64) merge_factor_kernel<double><<<grid, 128, 0, st>>>(S);
+    else merge_factor_kernel<float><<<grid, 128, 0, st>>>(S);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LUSP_OK : cuda_fail(e, "merge factor launch");
+}
+
 // ---------------------------------------------------------------------------
 // Patterns
 // ---------------------------------------------------------------------------
@@ -238,13 +272,26 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     PatternObj* P = new PatternObj();
     build_static_pattern(n, Ap, Ai, q.data(), F, 256, P->S, dense_tail);
     const StaticPattern& S = P->S;
+    // Bit pattern of the dense trailing block (see PatternDev::tail_mask).
+    std::vector<int> tail_mask;
+    if (S.dtail > 0) {
+        const int ldw = tail_ld(S) / 32;
+        tail_mask.assign((size_t)S.dtail * ldw, 0);
+        for (int k = S.k0; k < n; k++)
+            for (int p = S.cp[k]; p < S.cp[k + 1]; p++) {
+                const int r = S.ri[p];
+                if (r < S.k0) continue;
+                const int c = k - S.k0;
+                tail_mask[(size_t)(r - S.k0) * ldw + c / 32] |= (int)(1u << (c & 31));
+            }
+    }
 
     // One device block for every int array of the layout.
     const std::vector<int>* arrays[] = {&S.cp, &S.ri, &S.dg, &S.col_order, &S.a_ptr, &S.a_src, &S.a_dst,
                                         &S.lrp, &S.lci, &S.urp, &S.uci, &S.slot_dst, &S.fwd_order,
                                         &S.bwd_order, &S.sell_ptr, &S.sell_col, &S.sell_src,
                                         &S.sell_perm, &S.rowat, &S.q, &S.fwd_lev, &S.bwd_lev, &S.bwd_pos,
-                                        &S.fwd_ldesc, &S.bwd_ldesc, &S.dep_bc, &S.a_diag};
+                                        &S.fwd_ldesc, &S.bwd_ldesc, &S.dep_bc, &S.a_diag, &tail_mask};
     const int narr = (int)(sizeof(arrays) / sizeof(arrays[0]));
     std::vector<size_t> off(narr + 1, 0);
     // Each array gets at least 8 ints of slack: the sweeps copy index runs
@@ -296,6 +343,8 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     D.bwd_ldesc = blk + off[idx++];
     D.dep_bc = (const int2*)(blk + off[idx++]);
     D.a_diag = blk + off[idx++];
+    D.tail_mask = S.dtail > 0 ? (const unsigned*)(blk + off[idx]) : nullptr;
+    idx++;
     D.lev_max_ent = S.lev_max_ent;
     D.lev_max_rows = S.lev_max_rows;
     D.nfwd_levels = S.nfwd_levels;

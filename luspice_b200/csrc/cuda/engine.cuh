@@ -48,6 +48,11 @@ struct PatternDev {
     // Dense trailing block: rows/columns [k0, n), dtail = n - k0 (0: none),
     // stored row-major with leading dimension tail_ld.
     int k0, dtail, tail_ld;
+    // Pattern of the dense trailing block, one bit per entry (row r, column c
+    // of the block: bit c & 31 of word r * (tail_ld / 32) + c / 32).  The
+    // refactor writes only these entries of the fp64 block; the dense kernel
+    // reads every other entry as 0 in its first panel step.
+    const unsigned* tail_mask;
     const int* a_diag;       // [n] slot offset of A(q_k, q_k) in column k, or -1
     const int* bwd_pos;      // [n] row -> index in bwd_order
     const int* fwd_ldesc;    // [nfwd_levels * 5] level descriptors (see host)

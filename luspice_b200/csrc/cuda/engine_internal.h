@@ -138,6 +138,9 @@ int tail_ld(const StaticPattern& S);
 char* carve_system(SysDev& D, char* p, const StaticPattern& S, size_t vs, int m);
 size_t spill_bytes(int grid, int block, int colmax, const SmemPlan& rplan);
 int launch_systems(const LaunchArgs& a, cudaStream_t st);
+// Completes the merged slot array of one system (U part, diagonal, dense
+// block) on stream st.
+int batch_merge_factor(BatchObj* B, int sys, cudaStream_t st);
 int sm_count();
 // Loads every engine kernel into the current context now (not lazily at
 // its first launch).

@@ -140,6 +140,15 @@ __device__ void cta_store_pivot_stats(SysStats* st, Smem& sm, double minpiv, dou
 // the stored multiplier and the fp64 U value, so the factor equals the
 // column engine's bit for bit.  Pivot statistics as in the column engine.
 // ---------------------------------------------------------------------------
+// Entry (r, c) of the dense trailing block W, or 0 when it is outside the
+// block's pattern (first panel step only: the refactor wrote the pattern
+// entries alone, the rest of W holds whatever an earlier launch left).
+__device__ __forceinline__ double tail_entry(const double* W, int ld, const unsigned* mask, int r, int c,
+                                             bool masked) {
+    if (masked && !((__ldg(mask + (size_t)r * (ld >> 5) + (c >> 5)) >> (c & 31)) & 1u)) return 0.0;
+    return W[(size_t)r * ld + c];
+}
+
 template <typename VT>
 __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, const SmemPlan& plan,
                                   const SolveParams& prm, double& minpiv, double& minratio, int& bad,
@@ -155,11 +164,13 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
         ctr[0] = ctr[1] = ctr[2] = 0;
         ctr[3] = clock64();
     }
+    const unsigned* mask = P.tail_mask;
     for (int jb = 0; jb < D; jb += nb) {
         const int w = min(nb, D - jb), R = D - jb;
+        const bool first = jb == 0;
         for (int t = tid; t < R * nb; t += nt) {
             const int r = t / nb, c = t - r * nb;
-            pan[r * ps + c] = c < w ? W[(size_t)(jb + r) * ld + jb + c] : 0.0;
+            pan[r * ps + c] = c < w ? tail_entry(W, ld, mask, jb + r, jb + c, first) : 0.0;
         }
         if (tid < nb) cmax[tid] = 0ull;
         __syncthreads();
@@ -232,7 +243,7 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
             for (int g = 0; g < w; g += 8) {
                 double u[8];
 #pragma unroll
-                for (int r = 0; r < 8; r++) u[r] = g + r < w ? W[(size_t)(jb + g + r) * ld + col] : 0.0;
+                for (int r = 0; r < 8; r++) u[r] = g + r < w ? tail_entry(W, ld, mask, jb + g + r, (int)col, first) : 0.0;
                 for (int g2 = 0; g2 < g; g2 += 8) {
                     double v[8];
 #pragma unroll
@@ -283,7 +294,7 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
 #pragma unroll
                     for (int j = 0; j < 4; j++) {
                         const int col = q0 + lane + 32 * j;
-                        acc[q][j] = (row < D && col < D) ? W[(size_t)row * ld + col] : 0.0;
+                        acc[q][j] = (row < D && col < D) ? tail_entry(W, ld, mask, row, col, first) : 0.0;
                     }
                 }
                 const double* l0 = pan + (size_t)(rw - jb) * ps;
@@ -324,8 +335,8 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
 }
 
 // Dense trailing block -> VT storage for the solves (unit L below the
-// diagonal, U on and above) and the merged / row-major slot arrays of the
-// tail columns' rows >= k0.
+// diagonal, U on and above).  The block's entries live only there (the
+// merged slot array gets them from merge_factor_kernel when a caller asks).
 template <typename VT>
 __device__ void dense_tail_store(const SysDev& S, const PatternDev& P, const double* W, double& maxu,
                                  char* smem_tail_tiles, int ttw) {
@@ -359,24 +370,7 @@ __device__ void dense_tail_store(const SysDev& S, const PatternDev& P, const dou
         }
     }
     __syncthreads();
-    VT* lu = (VT*)S.lu;
-    VT* lval = (VT*)S.lval;
-    VT* uval = (VT*)S.uval;
-    VT* udiag = (VT*)S.udiag;
-    for (int kk = warp; kk < D; kk += nw) {
-        const int k = k0 + kk;
-        const int c0 = P.cp[k], len = P.cp[k + 1] - c0, d = P.dg[k] - c0;
-        const int* rows = P.ri + c0;
-        int below = 0;
-        for (int t = lane; t < d; t += 32) below += rows[t] < k0;
-        below = __reduce_add_sync(0xffffffffu, below);
-        for (int t = below + lane; t < len; t += 32) {
-            const VT sv = T[(size_t)kk * ld + (rows[t] - k0)];
-            lu[c0 + t] = sv;
-            if (t == d) udiag[k] = sv;
-            // Other slots of the block live only in the dense copy.
-        }
-    }
+    (void)k0;
 }
 
 // The dense trailing block of one system (its own kernel: few warps, many
@@ -452,19 +446,9 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
             sm.ctl[3] = 0;
         }
     }
-    const int gt = (int)(crank * blockDim.x + threadIdx.x), gs = (int)(csize * blockDim.x);
-    // A in SELL order for the solves: fp64 (outer residual) and fp32 (inner).
-    for (int t = gt; t < P.sell_total; t += gs) {
-        const int s = P.sell_src[t];
-        const double v = s >= 0 ? S.a_val[s] : 0.0;
-        S.sell64[t] = v;
-        S.sell32[t] = (float)v;
-    }
-    // The system's dense trailing block, zeroed: the tail columns scatter
-    // only their pattern's entries into it.
+    // The system's dense trailing block: the tail columns scatter their
+    // pattern's entries into it (the dense kernel reads the others as 0).
     double* W = P.dtail > 0 ? S.tailw : nullptr;
-    if (W)
-        for (size_t t = gt; t < (size_t)P.dtail * P.tail_ld; t += gs) W[t] = 0.0;
 
     VT* lu = (VT*)S.lu;
     VT* lval = (VT*)S.lval;
@@ -668,9 +652,7 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 const double v = x[t];
                 if (t < dsp) {
                     maxu = fmax(maxu, fabs(v));
-                    const VT sv = ValTraits<VT>::to(v);
-                    lu[c0 + t] = sv;
-                    uval[P.slot_dst[c0 + t]] = sv;
+                    uval[P.slot_dst[c0 + t]] = ValTraits<VT>::to(v);
                 } else {
                     W[(size_t)(rows[t] - P.k0) * P.tail_ld + (k - P.k0)] = v;
                 }
@@ -691,19 +673,24 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         const double ratio = amax > ap ? ap / amax : 1.0;
         minratio = fmin(minratio, ratio);
         if (ratio < prm.pivot_tol) bad |= ST_PIVOT_WEAK;
+        // Each value is stored once where the solves read it (U rows, the
+        // diagonal, L rows); the strict-L part also goes to the merged
+        // columns, which the later columns' gathers read.
         for (int t = lane; t < len; t += 32) {
             const int slot = c0 + t;
             double v = x[t];
             if (t > d) v = __ddiv_rn(v, piv);
             else maxu = fmax(maxu, fabs(v));
             const VT sv = ValTraits<VT>::to(v);
-            lu[slot] = sv;
             const int dst = P.slot_dst[slot];
             if (t < d) uval[dst] = sv;
             else if (t == d) {
                 udiag[k] = sv;
                 ((VT*)S.udiag_bwd)[P.bwd_pos[k]] = ValTraits<VT>::to(1.0 / piv);
-            } else lval[dst] = sv;
+            } else {
+                lu[slot] = sv;
+                lval[dst] = sv;
+            }
         }
         // Release: the column's values before its ready bit.
         share_fence(csize);
@@ -1287,6 +1274,19 @@ __device__ __forceinline__ double cta_dot(const double* a, const double* b, int 
     return block_sum(s, sm.red);
 }
 
+// A in SELL order for the solve's products, from the system's input
+// values: fp64 (outer residual, direct-solve residual) and, when the inner
+// products use it, fp32.  Ends with a CTA barrier.
+__device__ void build_sell_values(const SysDev& S, const PatternDev& P, bool f32) {
+    for (int t = threadIdx.x; t < P.sell_total; t += blockDim.x) {
+        const int s = P.sell_src[t];
+        const double v = s >= 0 ? S.a_val[s] : 0.0;
+        S.sell64[t] = v;
+        if (f32) S.sell32[t] = (float)v;
+    }
+    __syncthreads();
+}
+
 // Direct solve x = Q U^-1 L^-1 P b with the stored factors, then the fp64
 // residual of the result.
 template <typename VT>
@@ -1302,7 +1302,7 @@ __device__ void direct_phase(const SysDev& S, const SmemPlan& plan, char* smem_b
     int bad = 0;
     if (threadIdx.x == 0) S.stats->status &= ~kSolveBits;
     for (int i = threadIdx.x; i < n; i += blockDim.x) bt[i] = S.b[P.rowat[i]];
-    __syncthreads();
+    build_sell_values(S, P, false);
     const int* desc = nullptr;
     if (sweep_desc_fits(P, plan)) {
         int* d = sweep_desc_base(plan, sm);
@@ -1380,6 +1380,7 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         bt[i] = S.b[P.rowat[i]];
         xt[i] = 0.0;
     }
+    build_sell_values(S, P, sizeof(AT) != 8);
     const int* desc = nullptr;
     if (sweep_desc_fits(P, plan)) {
         int* d = sweep_desc_base(plan, sm);
