@@ -117,7 +117,8 @@ typedef struct {
                                       (1 or 2 with the same rule) */
     int solve_sweep;               /* triangular solves: 0 auto, 1 dataflow (per-row
                                       ready bits), 2 level-synchronous (barrier per
-                                      level, descriptors in shared memory) */
+                                      level; descriptors in shared memory when they
+                                      fit, else read from global memory) */
     int refactor_mode;             /* gathers of dependency columns: 0 staged in
                                       shared memory by asynchronous copies with
                                       precomputed relative slots, 1 loaded per
@@ -155,6 +156,13 @@ typedef struct {
     double factor_shift;           /* factor A + factor_shift diag|A(i,i)| instead of A
                                       (the residual still uses A; default 0) */
     double hard_shift;             /* the P-hard rung's shift (default 1e-7) */
+    int refactor_spread;           /* CTAs that share one system's refactorization
+                                      anywhere on the GPU, synchronizing through
+                                      global memory, for batches of a few large
+                                      systems: 0 auto (every SM for a batch of at
+                                      most SMs / 8 systems with at least 16 M
+                                      gathered updates each), -1 never, > 0 that
+                                      many CTAs per system (at most SMs / nsys) */
 } lusp_batch_opts;
 
 /* ---- library ---- */

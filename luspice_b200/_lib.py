@@ -43,7 +43,7 @@ class BatchOpts(C.Structure):
                 ("solve_sweep", C.c_int), ("refactor_mode", C.c_int), ("inner_prec", C.c_int),
                 ("xtol", C.c_double), ("refactor_threads", C.c_int),
                 ("refactor_cluster", C.c_int), ("ladder", C.c_int), ("ladder_slots", C.c_int),
-                ("factor_shift", C.c_double), ("hard_shift", C.c_double)]
+                ("factor_shift", C.c_double), ("hard_shift", C.c_double), ("refactor_spread", C.c_int)]
 
 
 class ServerOpts(C.Structure):

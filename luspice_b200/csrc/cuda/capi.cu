@@ -162,6 +162,7 @@ void lusp_batch_opts_default(lusp_batch_opts* o) {
     o->xtol = 1e-8;
     o->refactor_threads = 0;
     o->refactor_cluster = 0;
+    o->refactor_spread = 0;
     o->ladder = 0;
     o->ladder_slots = 0;
     o->factor_shift = 0.0;

@@ -64,10 +64,20 @@ __device__ __forceinline__ int item_count(int nsys, const int* dyn) {
 template <typename VT, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1)
 refactor_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan, SolveParams prm,
-                const int* dyn, const int* list) {
+                const int* dyn, const int* list, SpreadArgs sp) {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_task;
     const int ns = item_count(nsys, dyn);
+    if (sp.group > 0) {
+        // Spread mode: CTAs [t * group, (t + 1) * group) share system t.
+        const int t = (int)blockIdx.x / sp.group;
+        if (t < ns) {
+            const SysDev S = sys[list ? list[t] : t];
+            refactor_phase<VT, true>(S, plan, smem, prm, sp.sync + (size_t)t * sp.stride,
+                                     (int)blockIdx.x % sp.group, sp.group);
+        }
+        return;
+    }
     // A thread-block cluster (or a lone CTA) takes one system at a time:
     // rank 0 draws it, every CTA reads it through distributed shared memory
     // between two cluster barriers (so rank 0 outlives the read).
@@ -430,10 +440,12 @@ void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm,
     const size_t dneed = 4 * (size_t)nmax + (size_t)levmax + 8 + 5 * (size_t)levmax + 16;
     plan.dcap = (plan.ycap && (size_t)nmax * 8 + dneed * 4 <= avail) ? (int)dneed : 0;
     // Stage ring of the level sweeps: the widest level, or as many entries
-    // as fit (at least 256; wider levels then read global memory).
+    // as fit (at least 256; wider levels then read global memory).  Also
+    // when the solve vector or the descriptors stay in global memory (large
+    // systems): the sweeps then read the pattern's descriptors from there.
     plan.sc_ent = 0;
     plan.sc_rows = 0;
-    if (plan.dcap) {
+    {
         const size_t used = sweep_desc_offset(plan.ycap, m) - hbytes + (((size_t)plan.dcap + 3) & ~(size_t)3) * 4;
         const size_t left = avail > used ? avail - used : 0;
         int ce = (entmax + 3) & ~3, cr = (rowmax + 3) & ~3;
@@ -463,7 +475,8 @@ int refactor_block(const lusp_batch_opts& o, int nsys) {
     return nsys <= sm_count() ? 768 : 512;
 }
 
-void make_refactor_plan(const std::vector<PatternObj*>& pats, int threads, int vsize, SmemPlan& plan) {
+void make_refactor_plan(const std::vector<PatternObj*>& pats, int threads, int vsize, SmemPlan& plan,
+                        int ctas_per_sm) {
     int nmax = 1, colmax = 2;
     for (auto* p : pats) {
         nmax = std::max(nmax, p->S.n);
@@ -471,8 +484,8 @@ void make_refactor_plan(const std::vector<PatternObj*>& pats, int threads, int v
     }
     colmax = (colmax + 1) & ~1;
     // Target 32 resident warps per SM: one 1024-thread CTA, or several
-    // smaller ones.
-    const int ctas = std::max(1, 1024 / threads);
+    // smaller ones (or the given number of CTAs per SM).
+    const int ctas = ctas_per_sm > 0 ? ctas_per_sm : std::max(1, 1024 / threads);
     size_t budget = std::min<size_t>(227 * 1024, 228 * 1024 / ctas - 1024);
     plan.nwords = (nmax + 31) / 32;
     plan.m = 0;
@@ -548,7 +561,7 @@ static int kernel_prepare(size_t smem, int block, int* occ) {
     return prepare_kernel(solve_kernel<VT, AT>, smem, block, occ, &granted, mu);
 }
 
-using RefactorFn = void (*)(const SysDev*, int, int*, SmemPlan, SolveParams, const int*, const int*);
+using RefactorFn = void (*)(const SysDev*, int, int*, SmemPlan, SolveParams, const int*, const int*, SpreadArgs);
 
 // The refactor instance for a CTA of block threads: one CTA per SM above
 // 512 threads (the instance with the most registers that still fits the
@@ -631,15 +644,17 @@ int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ) {
 struct RungShape {
     SmemPlan rplan, dplan, plan;
     int rblock, rgrid, rcluster, dblock, dgrid, block, grid;
+    SpreadArgs rspread;
 };
 
 static RungShape main_shape(const LaunchArgs& a) {
-    return RungShape{a.rplan, a.dplan, a.plan, a.rblock, a.rgrid, a.rcluster, a.dblock, a.dgrid, a.block, a.grid};
+    return RungShape{a.rplan, a.dplan, a.plan, a.rblock, a.rgrid, a.rcluster, a.dblock, a.dgrid, a.block, a.grid,
+                     a.rspread};
 }
 
 static RungShape ladder_shape(const LaunchArgs& a) {
     return RungShape{a.xrplan, a.xdplan, a.xplan, a.xrblock, a.xrgrid, a.xrcluster, a.xdblock, a.xdgrid,
-                     a.xblock, a.xgrid};
+                     a.xblock, a.xgrid, a.xrspread};
 }
 
 // Refactor, dense-block and solve kernels of one rung over sys[0, nsys) (or
@@ -656,6 +671,12 @@ static int launch_rung(const SysDev* sys, int nsys, int* q, const int* dyn, cons
     if (what & LUSP_RUN_REFACTOR) {
         int rc = refactor_prepare<VT>(r.rplan.bytes, r.rblock, nullptr);
         if (rc != LUSP_OK) return rc;
+        if (r.rspread.group > 0) {
+            // The systems' sync areas start at zero (claim counters, status
+            // words, accumulators, ready bits).
+            e = cudaMemsetAsync(r.rspread.sync, 0, (size_t)nsys * r.rspread.stride * sizeof(unsigned), st);
+            if (e != cudaSuccess) return cuda_fail(e, "refactor sync reset");
+        }
         if (r.rcluster > 1) {
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3((unsigned)r.rgrid);
@@ -669,10 +690,11 @@ static int launch_rung(const SysDev* sys, int nsys, int* q, const int* dyn, cons
             attr[0].val.clusterDim.z = 1;
             cfg.attrs = attr;
             cfg.numAttrs = 1;
-            e = cudaLaunchKernelEx(&cfg, refactor_fn<VT>(r.rblock), sys, nsys, q, r.rplan, prm, dyn, list);
+            e = cudaLaunchKernelEx(&cfg, refactor_fn<VT>(r.rblock), sys, nsys, q, r.rplan, prm, dyn, list,
+                                   r.rspread);
         } else {
             refactor_fn<VT>(r.rblock)<<<r.rgrid, r.rblock, r.rplan.bytes, st>>>(sys, nsys, q, r.rplan, prm, dyn,
-                                                                             list);
+                                                                             list, r.rspread);
             e = cudaGetLastError();
         }
         if (e != cudaSuccess) return cuda_fail(e, "refactor kernel launch");
@@ -813,6 +835,12 @@ void fill_params(SolveParams& prm, const lusp_batch_opts& o) {
     prm.shift = o.factor_shift;
 }
 
+// Gathered updates per system above which a batch of few systems spreads
+// each system's refactorization over many SMs (the n = 40,000 circuit has
+// 227 M; the n = 4050 power grid, refactored faster by one 2-SM cluster,
+// has 5.9 M).
+constexpr long long kSpreadMinUpdates = 16ll << 20;
+
 int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, int nsys, LaunchArgs& a) {
     a.rblock = refactor_block(o, nsys);
     make_refactor_plan(pats, a.rblock, o.prec == LUSP_FP64 ? 8 : 4, a.rplan);
@@ -835,6 +863,50 @@ int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& 
         if (ncl >= 1 && (o.refactor_cluster > 1 || ncl >= nsys)) {
             a.rcluster = want;
             a.rgrid = want * std::min(nsys, ncl);
+        }
+    }
+    // Spread mode: a few large systems, each refactored by many CTAs that
+    // synchronize through global memory (the sync area is bound by the
+    // caller: batch_build).
+    a.rspread = SpreadArgs{};
+    if (o.refactor_spread >= 0) {
+        long long gmin = -1;
+        int nmax = 1;
+        for (auto* p : pats) {
+            gmin = gmin < 0 ? p->S.gathered : std::min<long long>(gmin, p->S.gathered);
+            nmax = std::max(nmax, p->S.n);
+        }
+        const int slots = occ * sm_count();
+        int g = 0;
+        if (o.refactor_spread > 0) g = std::min(o.refactor_spread, slots / std::max(1, nsys));
+        else if (nsys * 8 <= sm_count() && gmin >= kSpreadMinUpdates) g = slots / nsys;
+        if (g >= 2 && o.refactor_threads <= 0) {
+            // One CTA per SM, of the size whose per-warp work area holds the
+            // longest column before the dense block (longer ones spill to
+            // global memory).
+            int colsp = 2;
+            for (auto* p : pats)
+                for (int k = 0; k < p->S.k0; k++) colsp = std::max(colsp, p->S.cp[k + 1] - p->S.cp[k]);
+            const int vs = o.prec == LUSP_FP64 ? 8 : 4;
+            for (int t : {768, 512, 384, 256}) {
+                SmemPlan pl;
+                make_refactor_plan(pats, t, vs, pl, 1);
+                if (pl.wcap >= colsp || t == 256) {
+                    a.rblock = t;
+                    a.rplan = pl;
+                    break;
+                }
+            }
+            rc = refactor_occupancy(o.prec, a.rplan.bytes, a.rblock, &occ);
+            if (rc != LUSP_OK) return rc;
+            if (occ < 1) { set_error("refactor kernel does not fit one SM (smem %zu)", a.rplan.bytes); return LUSP_EARG; }
+            g = std::max(1, std::min(g, occ * sm_count() / nsys));
+        }
+        if (g >= 2) {
+            a.rspread.group = g;
+            a.rspread.stride = sync_stride(nmax);
+            a.rcluster = 1;
+            a.rgrid = g * nsys;
         }
     }
     // Dense trailing blocks: their own kernel when any system has one.
@@ -863,6 +935,7 @@ int ladder_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o,
     lusp_batch_opts x = o;
     x.prec = LUSP_FP64;
     x.inner_prec = 0;
+    x.refactor_spread = -1;
     x.block_threads = 0;
     x.ctas_per_sm = 0;
     resolve_solve_shape(x, cap);
@@ -937,8 +1010,8 @@ int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, Sme
         plan.dcap = 0;
         plan.sc_ent = plan.sc_rows = 0;
     }
-    if (o.solve_sweep == 2 && (plan.dcap == 0 || plan.sc_ent == 0)) {
-        set_error("level-synchronous sweeps need the solve vector and descriptors in shared memory");
+    if (o.solve_sweep == 2 && plan.sc_ent == 0) {
+        set_error("level-synchronous sweeps need a stage ring in shared memory");
         return LUSP_EARG;
     }
     return LUSP_OK;
@@ -990,7 +1063,9 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     rc = ladder_setup(B->pats, *o, ladder_cap(*o, nsys), a, lp);
     if (rc != LUSP_OK) { delete B; return rc; }
     const size_t spill = spill_bytes(a.rgrid, a.rblock, colmax, a.rplan);
-    const size_t total = base[nsys] + spill + al256(sizeof(SysStats) * nsys) + al256(sizeof(SysDev) * nsys) + 256;
+    const size_t syncb = a.rspread.group > 0 ? al256((size_t)nsys * a.rspread.stride * sizeof(unsigned)) : 0;
+    const size_t total =
+        base[nsys] + spill + al256(sizeof(SysStats) * nsys) + al256(sizeof(SysDev) * nsys) + 256 + syncb;
     char* blk = nullptr;
     cudaError_t e = cudaMalloc(&blk, total);
     if (e != cudaSuccess) { delete B; return cuda_fail(e, "batch device alloc"); }
@@ -1002,6 +1077,7 @@ int batch_build(int nsys, PatternObj* const* pats, const lusp_batch_opts* o, Bat
     B->d_stats = (SysStats*)stats_base;
     B->d_sys = (SysDev*)(stats_base + al256(sizeof(SysStats) * nsys));
     B->d_queue = (int*)((char*)B->d_sys + al256(sizeof(SysDev) * nsys));
+    if (syncb) a.rspread.sync = (unsigned*)((char*)B->d_queue + 256);
     double* spill_ptr = spill ? (double*)(blk + base[nsys]) : nullptr;
     B->d_vals = (double*)blk;
     B->d_rhs = (double*)(blk + al256(B->val_off[nsys] * 8));

@@ -193,6 +193,22 @@ struct EscDev {
     double rtol;             // ... as does a final residual above rtol
 };
 
+// Several CTAs per system for the refactorization of batches of few large
+// systems ("spread" mode): CTAs [s * group, (s + 1) * group) take the
+// columns of system s.  The claim counter, status words and ready bits of a
+// system live in global memory (its sync area, zeroed before the kernel):
+// words [0, 16) control (kSync* below), words [16, 32) eight 64-bit
+// accumulators of the pivot statistics and cycle counters, words [32, ...)
+// the ready bits.
+struct SpreadArgs {
+    int group;               // CTAs per system (0: cluster / queue mode)
+    unsigned* sync;          // sync areas of the systems
+    int stride;              // 32-bit words per system
+};
+constexpr int kSyncClaim = 0, kSyncStatus = 1, kSyncSingular = 2, kSyncAbort = 3, kSyncDone = 4;
+constexpr int kSyncAcc = 16, kSyncReady = 32;
+__host__ __device__ inline int sync_stride(int nmax) { return (kSyncReady + (nmax + 31) / 32 + 7) & ~7; }
+
 // Shared-memory plan of one launch (same for every CTA).
 struct SmemPlan {
     int nwords;              // ready-bit words (>= ceil(n_max/32))

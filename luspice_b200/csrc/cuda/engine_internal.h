@@ -41,6 +41,7 @@ struct LaunchArgs {
     int rblock = 1024;
     int rgrid = 1;
     int rcluster = 1;                // CTAs per system (thread-block cluster)
+    SpreadArgs rspread{};            // CTAs per system in global-memory sync (group 0: off)
     SmemPlan dplan{};                // dense trailing-block kernel (dgrid 0: none)
     int dblock = 512;
     int dgrid = 0;
@@ -50,6 +51,7 @@ struct LaunchArgs {
     EscDev esc{};
     SmemPlan xplan{}, xrplan{}, xdplan{};
     int xblock = 512, xgrid = 0, xrblock = 1024, xrgrid = 0, xrcluster = 1, xdblock = 512, xdgrid = 0;
+    SpreadArgs xrspread{};           // always off for the ladder
     SolveParams xprm{};              // P-safe parameters; P-hard adds the shift
     double hard_shift = 1e-7;
 };
@@ -126,7 +128,9 @@ int refactor_occupancy(int prec, size_t smem, int block, int* occ);
 int refactor_block(const lusp_batch_opts& o, int nsys);
 // Solve-kernel CTA size and plan target for nsys systems when left at 0.
 void resolve_solve_shape(lusp_batch_opts& o, int nsys);
-void make_refactor_plan(const std::vector<PatternObj*>& pats, int threads, int vsize, SmemPlan& plan);
+// ctas_per_sm: CTAs sharing an SM's shared memory (0: 1024 / threads).
+void make_refactor_plan(const std::vector<PatternObj*>& pats, int threads, int vsize, SmemPlan& plan,
+                        int ctas_per_sm = 0);
 // Refactorization kernel block, plan and grid for nsys systems of pats.
 int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, int nsys, LaunchArgs& a);
 // Kernels one launch with these RUN_* flags issues.

@@ -67,6 +67,12 @@ __device__ __forceinline__ void share_fence(unsigned csize) {
     if (csize > 1) asm volatile("fence.acq_rel.cluster;\n" ::: "memory");
     else __threadfence_block();
 }
+// GPU scope: CTAs on any SM share the system (spread mode).
+template <bool SPREAD>
+__device__ __forceinline__ void share_fence_t(unsigned csize) {
+    if (SPREAD) __threadfence();
+    else share_fence(csize);
+}
 
 __device__ __forceinline__ int warp_claim(int* counter) {
     int idx = 0;
@@ -415,9 +421,62 @@ __device__ __forceinline__ void cp_async_16(void* sdst, const void* gsrc) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 
-template <typename VT>
+// Spread mode: the pivot statistics and cycle counters of one CTA merged
+// into the system's sync area; the last CTA to finish writes the system's
+// statistics (pivot minima through the bit patterns of non-negative doubles:
+// a larger complement is a smaller value, so 0 means none yet).
+__device__ void spread_finish(const SysDev& S, unsigned* sync, int group, Smem& sm, double minpiv,
+                              double minratio, double maxu, int bad, long long cw, long long cg, long long cu,
+                              long long t_begin) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int* ctl = (int*)sync;
+    unsigned long long* acc = (unsigned long long*)(sync + kSyncAcc);
+    minpiv = warp_min(minpiv);
+    minratio = warp_min(minratio);
+    maxu = warp_max(maxu);
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if (lane == 0) {
+        if (bad) atomicOr(&ctl[kSyncStatus], bad);
+        if (minpiv < INFINITY) atomicMax(&acc[0], ~(unsigned long long)__double_as_longlong(minpiv));
+        if (minratio < INFINITY) atomicMax(&acc[1], ~(unsigned long long)__double_as_longlong(minratio));
+        atomicMax(&acc[2], (unsigned long long)__double_as_longlong(maxu));
+        atomicAdd(&acc[3], (unsigned long long)cw);
+        atomicAdd(&acc[4], (unsigned long long)cg);
+        atomicAdd(&acc[5], (unsigned long long)cu);
+    }
+    __threadfence();
+    __syncthreads();
+    (void)nw;
+    (void)sm;
+    if (threadIdx.x == 0 && atomicAdd(&ctl[kSyncDone], 1) == group - 1) {
+        __threadfence();
+        const volatile unsigned long long* va = acc;
+        const volatile int* vc = ctl;
+        SysStats* st = S.stats;
+        const unsigned long long a0 = va[0], a1 = va[1];
+        st->min_abs_pivot = a0 ? __longlong_as_double((long long)~a0) : INFINITY;
+        st->min_pivot_ratio = a1 ? __longlong_as_double((long long)~a1) : INFINITY;
+        st->max_abs_u = __longlong_as_double((long long)va[2]);
+        st->status = vc[kSyncStatus];
+        const int sc = vc[kSyncSingular];
+        st->singular_col = sc > 0 ? 0x7fffffff - sc : -1;
+        st->nres = 0;
+        st->inner_iters = 0;
+        st->outer_iters = 0;
+        st->cyc_wait = (long long)va[3];
+        st->cyc_gather = (long long)va[4];
+        st->cyc_update = (long long)va[5];
+        st->cyc_refactor = clock64() - t_begin;
+    }
+}
+
+// SPREAD: the system's columns are shared by `group` CTAs anywhere on the
+// GPU (CTA `member` of them) through the sync area in global memory; else
+// by the CTAs of this thread-block cluster through rank 0's shared memory.
+template <typename VT, bool SPREAD = false>
 __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem_base,
-                               const SolveParams& prm) {
+                               const SolveParams& prm, unsigned* sync = nullptr, int member = 0,
+                               int group = 1) {
     const PatternDev& P = *S.pat;
     const int n = P.n;
     Smem sm(smem_base, plan);
@@ -433,11 +492,12 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
     // rank 0's shared memory (distributed shared memory for the others).
     namespace cgr = cooperative_groups;
     cgr::cluster_group cl = cgr::this_cluster();
-    const unsigned crank = cl.block_rank(), csize = cl.num_blocks();
-    unsigned* ready = cl.map_shared_rank(sm.ready, 0);
-    int* ctl = cl.map_shared_rank(sm.ctl, 0);
+    const unsigned crank = SPREAD ? (unsigned)member : cl.block_rank();
+    const unsigned csize = SPREAD ? (unsigned)group : cl.num_blocks();
+    unsigned* ready = SPREAD ? sync + kSyncReady : cl.map_shared_rank(sm.ready, 0);
+    int* ctl = SPREAD ? (int*)sync : cl.map_shared_rank(sm.ctl, 0);
 
-    if (crank == 0) {
+    if (!SPREAD && crank == 0) {
         for (int t = threadIdx.x; t < (n + 31) / 32; t += blockDim.x) sm.ready[t] = 0u;
         if (threadIdx.x == 0) {
             sm.ctl[0] = 0;
@@ -458,12 +518,14 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
     int bad = 0;
     long long c_wait = 0, c_gather = 0, c_update = 0;
     const long long t_begin = clock64();
-    if (crank == 0 && threadIdx.x == 0) {
-        S.stats->cyc_wait = 0;
-        S.stats->cyc_gather = 0;
-        S.stats->cyc_update = 0;
+    if (!SPREAD) {
+        if (crank == 0 && threadIdx.x == 0) {
+            S.stats->cyc_wait = 0;
+            S.stats->cyc_gather = 0;
+            S.stats->cyc_update = 0;
+        }
+        cl.sync();
     }
-    cl.sync();
 
     while (true) {
         const int idx = warp_claim(&ctl[0]);
@@ -539,9 +601,9 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 bad |= ST_WAIT_TIMEOUT;
                 nready = 1;
             }
-            // Acquire: the dependency columns' values (written by any CTA of
-            // the cluster) are read after their ready bits.
-            share_fence(csize);
+            // Acquire: the dependency columns' values (written by any CTA
+            // sharing the system) are read after their ready bits.
+            share_fence_t<SPREAD>(csize);
             {
                 const long long t2 = clock64();
                 c_wait += t2 - tc;
@@ -667,7 +729,12 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         const double ap = fabs(piv);
         if (!(ap > 0.0) || !isfinite(piv)) {
             bad |= ST_SINGULAR;
-            if (lane == 0) atomicMin(&ctl[2], k);
+            // The first singular column: a minimum (spread mode: the sync
+            // area starts at 0, so the maximum of INT_MAX - k).
+            if (lane == 0) {
+                if (SPREAD) atomicMax(&ctl[kSyncSingular], 0x7fffffff - k);
+                else atomicMin(&ctl[2], k);
+            }
         }
         minpiv = fmin(minpiv, ap);
         const double ratio = amax > ap ? ap / amax : 1.0;
@@ -693,11 +760,15 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
             }
         }
         // Release: the column's values before its ready bit.
-        share_fence(csize);
+        share_fence_t<SPREAD>(csize);
         __syncwarp();
         if (lane == 0) set_ready(ready, k);
     }
 
+    if (SPREAD) {
+        spread_finish(S, sync, group, sm, minpiv, minratio, maxu, bad, c_wait, c_gather, c_update, t_begin);
+        return;
+    }
     if (lane == 0) {
         atomicAdd((unsigned long long*)&S.stats->cyc_wait, (unsigned long long)c_wait);
         atomicAdd((unsigned long long*)&S.stats->cyc_gather, (unsigned long long)c_gather);
@@ -922,10 +993,30 @@ __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.w
 // computed, so a level's work reads shared memory only.  A level's rows are
 // spread over groups of g lanes, g the power of two at or above its mean
 // row length (1..32): wide levels of short rows run a row per thread,
-// narrow levels of long rows a row per warp.  Levels larger than a stage
-// read global memory directly.
+// narrow levels of long rows a row per warp, or, for a level of a few very
+// long rows, several warps per row whose partial sums are added in warp
+// order (part: NT / 32 doubles of shared memory).  Levels larger than a
+// stage read global memory directly.
 // UPPER: y[i] = (y[i] - sum) / diag (U sweep), else y[i] -= sum.
 constexpr int kStages = 4;
+
+// sum over e = e0, e0 + g, ... < pe of val[e] * y[col[e]]: four partial
+// sums, so a lane has four loads of y in flight when y lives in global
+// memory (a row with fewer than four entries per lane keeps one sum).
+template <typename VT>
+__device__ __forceinline__ double row_dot(const VT* vv, const int* cc, const double* y, int e0, int pe, int g) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int e = e0;
+    for (; e + 3 * g < pe; e += 4 * g) {
+        const int c0 = cc[e], c1 = cc[e + g], c2 = cc[e + 2 * g], c3 = cc[e + 3 * g];
+        a0 = fma(ValTraits<VT>::load(vv + e), y[c0], a0);
+        a1 = fma(ValTraits<VT>::load(vv + e + g), y[c1], a1);
+        a2 = fma(ValTraits<VT>::load(vv + e + 2 * g), y[c2], a2);
+        a3 = fma(ValTraits<VT>::load(vv + e + 3 * g), y[c3], a3);
+    }
+    for (; e < pe; e += g) a0 = fma(ValTraits<VT>::load(vv + e), y[cc[e]], a0);
+    return (a0 + a1) + (a2 + a3);
+}
 
 __host__ __device__ inline size_t stage_bytes(int cap_e, int cap_r, int vsize) {
     return (size_t)(cap_e + 8) * (4 + vsize) + (size_t)(cap_r + 8) * vsize;
@@ -942,7 +1033,7 @@ __device__ __forceinline__ void sweep_barrier(int nthreads) {
 template <typename VT, bool UPPER>
 __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* lgl, const int* order, const int* rp,
                              const int* ci, const VT* val, const VT* dgo, double* y,
-                             char* stage, int cap_e, int cap_r) {
+                             char* stage, int cap_e, int cap_r, double* part) {
     const int NT = min((int)blockDim.x, kSweepThreads);
     if ((int)threadIdx.x >= NT) {
         __syncthreads();
@@ -991,7 +1082,39 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
         const VT* vv = st ? (const VT*)(base + (size_t)CE * 4) : val;
         const VT* dd = st ? (const VT*)(base + (size_t)CE * (4 + sizeof(VT))) : dgo;
         const int eb = st ? (d.z & ~3) : 0, rb = st ? (r0 & ~3) : 0;
-        const int lg = lgl[L], g = 1 << lg;
+        const int lgd = lgl[L];
+        if (lgd > 5) {
+            // Threads per row: the largest power of two (32 .. 2^lgd) that
+            // still gives every row of the level its own group in one pass.
+            int gw = 32;
+            while (gw * 2 <= (1 << lgd) && gw * 2 * nr <= NT) gw *= 2;
+            if (gw > 32) {
+                const int rpp = NT / gw, wpr = gw >> 5;
+                const int lane = threadIdx.x & 31;
+                for (int rp0 = r0; rp0 < r1; rp0 += rpp) {
+                    const int r = rp0 + (int)threadIdx.x / gw;
+                    const int lig = (int)threadIdx.x & (gw - 1);
+                    double acc = 0.0;
+                    if (r < r1) acc = row_dot<VT>(vv, cc, y, rp[r] - eb + lig, rp[r + 1] - eb, gw);
+                    acc = warp_sum(acc);
+                    if (lane == 0) part[warp] = acc;
+                    sweep_barrier(NT);
+                    if ((int)threadIdx.x < rpp) {
+                        const int rr = rp0 + (int)threadIdx.x;
+                        if (rr < r1) {
+                            double sum = 0.0;
+                            for (int w = 0; w < wpr; w++) sum += part[threadIdx.x * wpr + w];
+                            const int i = order[rr];
+                            if (UPPER) y[i] = (y[i] - sum) * ValTraits<VT>::load(dd + (rr - rb));
+                            else y[i] = y[i] - sum;
+                        }
+                    }
+                    sweep_barrier(NT);
+                }
+                continue;
+            }
+        }
+        const int lg = min(lgd, 5), g = 1 << lg;
         const int lig = threadIdx.x & (g - 1);
         const int ngr = NT >> lg;
         const int rounds = pow2 ? (nr + ngr - 1) >> (lgb - lg) : (nr + ngr - 1) / ngr;
@@ -1000,11 +1123,7 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
             if (rbase + ((warp * 32) >> lg) >= r1) break;   // nothing left for this warp
             const int r = rbase + ((int)threadIdx.x >> lg);
             double acc = 0.0;
-            if (r < r1) {
-                const int pe = rp[r + 1] - eb;
-                for (int e = rp[r] - eb + lig; e < pe; e += g)
-                    acc = fma(ValTraits<VT>::load(vv + e), y[cc[e]], acc);
-            }
+            if (r < r1) acc = row_dot<VT>(vv, cc, y, rp[r] - eb + lig, rp[r + 1] - eb, g);
             for (int o = g >> 1; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, g);
             if (r < r1 && lig == 0) {
                 const int i = order[r];
@@ -1038,6 +1157,20 @@ __device__ __forceinline__ int* sweep_desc_base(const SmemPlan& plan, Smem& sm) 
 struct SweepDesc {
     const int4 *f_ld, *b_ld;
     const int *f_lg, *b_lg, *f_ord, *f_rp, *b_ord, *b_rp;
+    // The pattern's own arrays in global memory (systems whose solve vector
+    // or descriptors do not fit shared memory).
+    __device__ explicit SweepDesc(const PatternDev& P) {
+        const int nfl = P.nfwd_levels, nbl = P.nbwd_levels;
+        f_ld = (const int4*)P.fwd_ldesc;
+        b_ld = (const int4*)P.bwd_ldesc;
+        f_lg = P.fwd_ldesc + 4 * nfl;
+        b_lg = P.bwd_ldesc + 4 * nbl;
+        f_ord = P.fwd_order;
+        f_rp = P.lrp;
+        b_ord = P.bwd_order;
+        b_rp = P.urp;
+    }
+    // The packed copy load_sweep_desc wrote to shared memory at d.
     __device__ SweepDesc(const PatternDev& P, const int* d) {
         const int n = P.n, nfl = P.nfwd_levels, nbl = P.nbwd_levels;
         f_ld = (const int4*)d;
@@ -1081,18 +1214,19 @@ __device__ __forceinline__ char* sweep_stage_base(const SmemPlan& plan, Smem& sm
     return (char*)(sweep_desc_base(plan, sm) + ((plan.dcap + 3) & ~3));
 }
 
-// y := U^-1 L^-1 rhs with the level-synchronous sweeps (descriptors already
-// in shared memory at d, stage ring at stage).
+// y := U^-1 L^-1 rhs with the level-synchronous sweeps (descriptors sd in
+// shared or global memory, stage ring at stage).  y may be global memory:
+// the sweep barriers order its writes and reads inside the CTA.
 template <typename VT>
 __device__ void cta_lu_apply_levels(const SysDev& S, const PatternDev& P, const SmemPlan& plan,
-                                    const double* rhs, double* y, const int* d, char* stage) {
+                                    const double* rhs, double* y, const SweepDesc& sd, char* stage,
+                                    double* part) {
     const int n = P.n;
-    const SweepDesc sd(P, d);
     for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = rhs[i];
     __syncthreads();
     const long long t0 = clock64();
     staged_sweep<VT, false>(P.nfwd_levels, sd.f_ld, sd.f_lg, sd.f_ord, sd.f_rp, P.lci, (const VT*)S.lval,
-                            nullptr, y, stage, plan.sc_ent, plan.sc_rows);
+                            nullptr, y, stage, plan.sc_ent, plan.sc_rows, part);
     const long long t1 = clock64();
     if (P.dtail > 0) {
         tail_forward<VT>(P, (const VT*)S.tail, y, S.stats);
@@ -1100,7 +1234,7 @@ __device__ void cta_lu_apply_levels(const SysDev& S, const PatternDev& P, const 
     }
     const long long t2 = clock64();
     staged_sweep<VT, true>(P.nbwd_levels, sd.b_ld, sd.b_lg, sd.b_ord, sd.b_rp, P.uci, (const VT*)S.uval,
-                           (const VT*)S.udiag_bwd, y, stage, plan.sc_ent, plan.sc_rows);
+                           (const VT*)S.udiag_bwd, y, stage, plan.sc_ent, plan.sc_rows, part);
     if (threadIdx.x == 0) {
         S.stats->cyc_lsolve += t1 - t0;
         S.stats->cyc_tail += t2 - t1;
@@ -1108,15 +1242,35 @@ __device__ void cta_lu_apply_levels(const SysDev& S, const PatternDev& P, const 
     }
 }
 
-// Dispatch: level-synchronous sweeps when their descriptors sit in shared
-// memory (desc != nullptr), else the dataflow version.
+// Dispatch: level-synchronous sweeps when the launch has a stage ring
+// (sd != nullptr: descriptors in shared memory when they fit, else read
+// from the pattern in global memory), else the dataflow version.
 template <typename VT>
 __device__ __forceinline__ void lu_apply(const SysDev& S, const SmemPlan& plan, const double* rhs,
-                                         double* y, Smem& sm, const int* desc, int& bad) {
+                                         double* y, Smem& sm, const SweepDesc* sd, int& bad) {
     const PatternDev& P = *S.pat;
-    if (desc) cta_lu_apply_levels<VT>(S, P, plan, rhs, y, desc, sweep_stage_base(plan, sm));
+    if (sd) cta_lu_apply_levels<VT>(S, P, plan, rhs, y, *sd, sweep_stage_base(plan, sm), sm.red);
     else cta_lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, (const VT*)S.tail, rhs,
                           y, sm, bad, S.stats);
+}
+
+// The sweep descriptors of a solve: loaded into shared memory when they fit
+// (returns the packed copy), else the pattern's global arrays when the
+// launch has a stage ring, else none (dataflow sweeps).  Ends with a CTA
+// barrier.
+__device__ const SweepDesc* prepare_sweeps(const PatternDev& P, const SmemPlan& plan, Smem& sm, SweepDesc* buf) {
+    const SweepDesc* sd = nullptr;
+    if (sweep_desc_fits(P, plan)) {
+        int* d = sweep_desc_base(plan, sm);
+        load_sweep_desc(P, d);
+        *buf = SweepDesc(P, d);
+        sd = buf;
+    } else if (plan.sc_ent > 0) {
+        *buf = SweepDesc(P);
+        sd = buf;
+    }
+    __syncthreads();
+    return sd;
 }
 
 // out = A x (RESID: out = bt - A x) with A in SELL-C-sigma, C = 32, values AT.
@@ -1303,12 +1457,8 @@ __device__ void direct_phase(const SysDev& S, const SmemPlan& plan, char* smem_b
     if (threadIdx.x == 0) S.stats->status &= ~kSolveBits;
     for (int i = threadIdx.x; i < n; i += blockDim.x) bt[i] = S.b[P.rowat[i]];
     build_sell_values(S, P, false);
-    const int* desc = nullptr;
-    if (sweep_desc_fits(P, plan)) {
-        int* d = sweep_desc_base(plan, sm);
-        load_sweep_desc(P, d);
-        desc = d;
-    }
+    SweepDesc sdb(P);
+    const SweepDesc* desc = prepare_sweeps(P, plan, sm, &sdb);
     const double nb = sqrt(cta_dot(bt, bt, n, sm));
     lu_apply<VT>(S, plan, bt, y, sm, desc, bad);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -1381,13 +1531,8 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
         xt[i] = 0.0;
     }
     build_sell_values(S, P, sizeof(AT) != 8);
-    const int* desc = nullptr;
-    if (sweep_desc_fits(P, plan)) {
-        int* d = sweep_desc_base(plan, sm);
-        load_sweep_desc(P, d);
-        desc = d;
-    }
-    __syncthreads();
+    SweepDesc sdb(P);
+    const SweepDesc* desc = prepare_sweeps(P, plan, sm, &sdb);
     bool use16 = false;
     if constexpr (kHalf) {
         // V holds nothing yet: its first n doubles serve the column maxima.

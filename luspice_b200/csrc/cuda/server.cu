@@ -349,6 +349,7 @@ bool ServerObj::try_launch(Flight& f) {
         if (kernel_occupancy(o.prec, o.inner_prec, plan.bytes, o.block_threads, &occ) != LUSP_OK || occ < 1)
             return false;
         grid = std::min(nsp, occ * sm_count());
+        o.refactor_spread = -1;   // the arenas hold no per-system sync areas
         if (refactor_setup(pats, o, nsp, la) != LUSP_OK) return false;
         spill = spill_bytes(la.rgrid, la.rblock, cm, la.rplan);
         // Device-side escalation of the mixed path: a few ladder slots with

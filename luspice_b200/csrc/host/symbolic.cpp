@@ -451,7 +451,8 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         }
         // Per-level descriptors of both sweeps: first row, end row, first
         // entry, end entry, and log2 of the lanes per row (the power of two
-        // at or above the level's mean row length, at most 32).
+        // at or above the level's mean row length, at most 512: above 32,
+        // several warps share a row when the level has few rows).
         auto level_desc = [](int nlev, const std::vector<int>& lev, const std::vector<int>& rp,
                              std::vector<int>& out) {
             out.assign((size_t)nlev * 5, 0);
@@ -461,7 +462,7 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
                 const int nr = std::max(1, r1 - r0);
                 const int mean = (e1 - e0 + nr - 1) / nr;
                 int lg = 0;
-                while ((1 << lg) < mean && lg < 5) lg++;
+                while ((1 << lg) < mean && lg < 9) lg++;
                 out[(size_t)l * 4 + 0] = r0;
                 out[(size_t)l * 4 + 1] = r1;
                 out[(size_t)l * 4 + 2] = e0;

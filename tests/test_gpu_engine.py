@@ -182,3 +182,59 @@ def test_cluster_refactor_bitwise(gpu, prec):
             assert np.array_equal(got.view(ity), exp.astype(got.dtype).view(ity))
         for k in ("min_abs_pivot", "min_pivot_ratio", "max_abs_u", "status", "singular_col"):
             assert out[0][1][s][k] == out[1][1][s][k], k
+
+
+@pytest.mark.parametrize("prec", [api.MIXED, api.FP64])
+@pytest.mark.parametrize("group", [2, 37])
+def test_refactor_spread_bitwise(gpu, prec, group):
+    """Spread mode (several CTAs anywhere on the GPU share each system's
+    columns through a claim counter and ready bits in global memory): the
+    factor is the host restatement's bit for bit, as in cluster mode, and
+    the pivot statistics equal the cluster mode's."""
+    m = small_problems()[1]
+    P = api.Pattern.from_matrix(m)
+    vals = m.perturbed(3, seed=31)
+    out = {}
+    for spread in (-1, group):
+        B = api.Batch([P] * 3, prec=prec, refactor_spread=spread)
+        B.upload(list(vals), [m.b] * 3)
+        B.run(api.RUN_BOTH)
+        out[spread] = ([B.factor_values(s) for s in range(3)], B.stats(), B.split(B.download()))
+        B.close()
+    _, q = P.perm()
+    for s in range(3):
+        got = out[group][0][s]
+        exp, bad = oracle_refactor(m, P, vals[s], fp32=(prec == api.MIXED))
+        exp = exp.astype(got.dtype)
+        ity = np.uint32 if got.dtype == np.float32 else np.uint64
+        assert np.array_equal(got.view(ity), exp.view(ity)), f"system {s}"
+        a, b = out[-1][1][s], out[group][1][s]
+        for key in ("min_abs_pivot", "min_pivot_ratio", "max_abs_u", "status", "singular_col"):
+            assert a[key] == b[key], (key, a[key], b[key])
+        assert np.array_equal(out[-1][2][s], out[group][2][s])
+        assert rel_err(out[group][2][s], oracle_solution(m, vals[s], q=q)) <= TOL_REL
+
+
+def test_refactor_spread_singular_column(gpu):
+    """A zero pivot found in spread mode is reported as the first singular
+    column, as in cluster mode."""
+    m = small_problems()[0]
+    P = api.Pattern.from_matrix(m)
+    cp, ri, dg = P.structure()
+    pinv, q = P.perm()
+    v = m.Ax.copy()
+    # Zero the whole input column that becomes pivot column k (its diagonal
+    # then receives only the updates, which are zero when the column is
+    # empty): pick a column with no dependencies.
+    k = next(k for k in range(m.n) if dg[k] == cp[k])
+    c = q[k]
+    v[m.Ap[c]:m.Ap[c + 1]] = 0.0
+    sts = {}
+    for spread in (-1, 5):
+        B = api.Batch([P], prec=api.FP64, refactor_spread=spread)
+        B.upload([v], [m.b])
+        B.run(api.RUN_REFACTOR)
+        sts[spread] = B.stats()[0]
+        B.close()
+    assert sts[5]["status"] & api.ST_SINGULAR
+    assert sts[5]["singular_col"] == sts[-1]["singular_col"] >= 0

@@ -63,3 +63,24 @@ def test_large_fp32_inner_stagnates_and_keeps_best(gpu, large):
     assert st["status"] & (api.ST_STAGNATED | api.ST_NOT_CONVERGED)
     r = np.linalg.norm(m.matvec(x) - m.b) / np.linalg.norm(m.b)
     assert r <= min(st["res"]) * (1 + 1e-6)
+
+
+def test_large_spread_and_wide_sweeps_match_single_cluster(gpu, large):
+    """The 40k system refactored by every SM (spread mode, the default for a
+    lone large system) gives the same factor bits as one 2-SM cluster, and
+    the level sweeps with several warps per long row give the same solution
+    class as the per-row dataflow sweeps."""
+    m, P, ref = large
+    xs, fv = {}, {}
+    for spread, sweep in ((0, 0), (-1, 1)):
+        B = api.Batch([P], prec=api.FP64, refactor_spread=spread, solve_sweep=sweep)
+        B.upload([m.Ax], [m.b])
+        B.run(api.RUN_BOTH)
+        xs[spread] = B.download()
+        fv[spread] = B.factor_values(0)
+        st = B.stats()[0]
+        assert st["status"] & api.ST_FAIL_MASK == 0, st
+        B.close()
+    assert np.array_equal(fv[0].view(np.uint64), fv[-1].view(np.uint64))
+    for k in xs:
+        assert rel_err(xs[k], ref) <= TOL_REL
