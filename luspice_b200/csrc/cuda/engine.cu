@@ -68,16 +68,7 @@ refactor_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan p
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_task;
     const int ns = item_count(nsys, dyn);
-    if (sp.group > 0) {
-        // Spread mode: CTAs [t * group, (t + 1) * group) share system t.
-        const int t = (int)blockIdx.x / sp.group;
-        if (t < ns) {
-            const SysDev S = sys[list ? list[t] : t];
-            refactor_phase<VT, true>(S, plan, smem, prm, sp.sync + (size_t)t * sp.stride,
-                                     (int)blockIdx.x % sp.group, sp.group);
-        }
-        return;
-    }
+    (void)sp;
     // A thread-block cluster (or a lone CTA) takes one system at a time:
     // rank 0 draws it, every CTA reads it through distributed shared memory
     // between two cluster barriers (so rank 0 outlives the read).
@@ -94,6 +85,23 @@ refactor_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan p
         const SysDev S = sys[list ? list[t] : t];
         refactor_phase<VT>(S, plan, smem, prm);
     }
+}
+
+// Spread mode (its own kernel, so the cluster kernel's register allocation
+// is its own): CTAs [t * group, (t + 1) * group) share system t, one CTA
+// per SM.
+template <typename VT, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
+refactor_spread_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan, SolveParams prm,
+                       const int* dyn, const int* list, SpreadArgs sp) {
+    extern __shared__ __align__(16) char smem[];
+    (void)queue;
+    const int ns = item_count(nsys, dyn);
+    const int t = (int)blockIdx.x / sp.group;
+    if (t >= ns) return;
+    const SysDev S = sys[list ? list[t] : t];
+    refactor_phase<VT, true>(S, plan, smem, prm, sp.sync + (size_t)t * sp.stride, (int)blockIdx.x % sp.group,
+                             sp.group);
 }
 
 template <typename VT>
@@ -282,6 +290,30 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     PatternObj* P = new PatternObj();
     build_static_pattern(n, Ap, Ai, q.data(), F, 256, P->S, dense_tail);
     const StaticPattern& S = P->S;
+    // Column records of the refactorization (see PatternDev::crec).
+    std::vector<int> crec((size_t)12 * n, 0);
+    for (int idx = 0; idx < n; idx++) {
+        const int k = S.col_order[idx];
+        int* r = crec.data() + (size_t)12 * idx;
+        const int c0 = S.cp[k], d = S.dg[k] - c0;
+        int dsp = d;
+        if (k >= S.k0) {
+            dsp = 0;
+            for (int t = 0; t < d; t++) dsp += S.ri[c0 + t] < S.k0;
+        }
+        const long long rp = S.rel_ptr.empty() ? 0 : S.rel_ptr[k];
+        r[0] = k;
+        r[1] = c0;
+        r[2] = S.cp[k + 1] - c0;
+        r[3] = d;
+        r[4] = S.a_ptr[k];
+        r[5] = S.a_ptr[k + 1];
+        r[6] = dsp;
+        r[7] = S.bwd_pos[k];
+        r[8] = (int)(unsigned)(rp & 0xffffffffll);
+        r[9] = (int)(unsigned)((unsigned long long)rp >> 32);
+        r[10] = S.a_diag[k];
+    }
     // Bit pattern of the dense trailing block (see PatternDev::tail_mask).
     std::vector<int> tail_mask;
     if (S.dtail > 0) {
@@ -301,7 +333,7 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
                                         &S.lrp, &S.lci, &S.urp, &S.uci, &S.slot_dst, &S.fwd_order,
                                         &S.bwd_order, &S.sell_ptr, &S.sell_col, &S.sell_src,
                                         &S.sell_perm, &S.rowat, &S.q, &S.fwd_lev, &S.bwd_lev, &S.bwd_pos,
-                                        &S.fwd_ldesc, &S.bwd_ldesc, &S.dep_bc, &S.a_diag, &tail_mask};
+                                        &S.fwd_ldesc, &S.bwd_ldesc, &S.dep_bc, &S.a_diag, &tail_mask, &crec};
     const int narr = (int)(sizeof(arrays) / sizeof(arrays[0]));
     std::vector<size_t> off(narr + 1, 0);
     // Each array gets at least 8 ints of slack: the sweeps copy index runs
@@ -355,6 +387,7 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     D.a_diag = blk + off[idx++];
     D.tail_mask = S.dtail > 0 ? (const unsigned*)(blk + off[idx]) : nullptr;
     idx++;
+    D.crec = (const int4*)(blk + off[idx++]);
     D.lev_max_ent = S.lev_max_ent;
     D.lev_max_rows = S.lev_max_rows;
     D.nfwd_levels = S.nfwd_levels;
@@ -567,7 +600,8 @@ using RefactorFn = void (*)(const SysDev*, int, int*, SmemPlan, SolveParams, con
 // 512 threads (the instance with the most registers that still fits the
 // block), else the 1024-thread instance, whose CTAs pack several per SM.
 template <typename VT>
-static RefactorFn refactor_fn(int block) {
+static RefactorFn refactor_fn(int block, bool spread = false) {
+    if (spread) return block <= 512 ? refactor_spread_kernel<VT, 1024> : refactor_spread_kernel<VT, 768>;
     if (block <= 512) return refactor_kernel<VT, 1024>;
     if (block <= 640) return refactor_kernel<VT, 640>;
     if (block <= 768) return refactor_kernel<VT, 768>;
@@ -575,11 +609,11 @@ static RefactorFn refactor_fn(int block) {
 }
 
 template <typename VT>
-static int refactor_prepare(size_t smem, int block, int* occ) {
+static int refactor_prepare(size_t smem, int block, int* occ, bool spread = false) {
     static std::mutex mu;
-    static size_t granted[3] = {0, 0, 0};   // per instance: 1024, 640, 768
-    const int slot = block <= 512 || block > 768 ? 0 : block <= 640 ? 1 : 2;
-    return prepare_kernel(refactor_fn<VT>(block), smem, block, occ, &granted[slot], mu);
+    static size_t granted[5] = {0, 0, 0, 0, 0};   // per instance: 1024, 640, 768, spread 1024, spread 768
+    const int slot = spread ? (block <= 512 ? 3 : 4) : block <= 512 || block > 768 ? 0 : block <= 640 ? 1 : 2;
+    return prepare_kernel(refactor_fn<VT>(block, spread), smem, block, occ, &granted[slot], mu);
 }
 
 // Clusters of csize refactor CTAs that can be resident at once.
@@ -617,7 +651,9 @@ int preload_kernels() {
     const void* fns[] = {
         (const void*)refactor_fn<float>(512), (const void*)refactor_fn<float>(640), (const void*)refactor_fn<float>(768),
         (const void*)refactor_fn<double>(512), (const void*)refactor_fn<double>(640),
-        (const void*)refactor_fn<double>(768), (const void*)dense_kernel<float>, (const void*)dense_kernel<double>,
+        (const void*)refactor_fn<double>(768), (const void*)refactor_fn<float>(768, true),
+        (const void*)refactor_fn<float>(512, true), (const void*)refactor_fn<double>(768, true),
+        (const void*)refactor_fn<double>(512, true), (const void*)dense_kernel<float>, (const void*)dense_kernel<double>,
         (const void*)solve_kernel<float, float>, (const void*)solve_kernel<float, double>,
         (const void*)solve_kernel<float, __half>, (const void*)solve_kernel<double, double>};
     for (const void* f : fns) {
@@ -628,9 +664,9 @@ int preload_kernels() {
     return LUSP_OK;
 }
 
-int refactor_occupancy(int prec, size_t smem, int block, int* occ) {
-    if (prec == LUSP_FP64) return refactor_prepare<double>(smem, block, occ);
-    return refactor_prepare<float>(smem, block, occ);
+int refactor_occupancy(int prec, size_t smem, int block, int* occ, bool spread) {
+    if (prec == LUSP_FP64) return refactor_prepare<double>(smem, block, occ, spread);
+    return refactor_prepare<float>(smem, block, occ, spread);
 }
 
 int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ) {
@@ -669,7 +705,8 @@ static int launch_rung(const SysDev* sys, int nsys, int* q, const int* dyn, cons
     cudaError_t e;
     if (kev && cudaEventRecord(kev[0], st) != cudaSuccess) return cuda_fail(cudaGetLastError(), "timing event");
     if (what & LUSP_RUN_REFACTOR) {
-        int rc = refactor_prepare<VT>(r.rplan.bytes, r.rblock, nullptr);
+        const bool spread = r.rspread.group > 0;
+        int rc = refactor_prepare<VT>(r.rplan.bytes, r.rblock, nullptr, spread);
         if (rc != LUSP_OK) return rc;
         if (r.rspread.group > 0) {
             // The systems' sync areas start at zero (claim counters, status
@@ -693,8 +730,8 @@ static int launch_rung(const SysDev* sys, int nsys, int* q, const int* dyn, cons
             e = cudaLaunchKernelEx(&cfg, refactor_fn<VT>(r.rblock), sys, nsys, q, r.rplan, prm, dyn, list,
                                    r.rspread);
         } else {
-            refactor_fn<VT>(r.rblock)<<<r.rgrid, r.rblock, r.rplan.bytes, st>>>(sys, nsys, q, r.rplan, prm, dyn,
-                                                                             list, r.rspread);
+            refactor_fn<VT>(r.rblock, spread)<<<r.rgrid, r.rblock, r.rplan.bytes, st>>>(sys, nsys, q, r.rplan, prm,
+                                                                                     dyn, list, r.rspread);
             e = cudaGetLastError();
         }
         if (e != cudaSuccess) return cuda_fail(e, "refactor kernel launch");
@@ -897,7 +934,7 @@ int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& 
                     break;
                 }
             }
-            rc = refactor_occupancy(o.prec, a.rplan.bytes, a.rblock, &occ);
+            rc = refactor_occupancy(o.prec, a.rplan.bytes, a.rblock, &occ, true);
             if (rc != LUSP_OK) return rc;
             if (occ < 1) { set_error("refactor kernel does not fit one SM (smem %zu)", a.rplan.bytes); return LUSP_EARG; }
             g = std::max(1, std::min(g, occ * sm_count() / nsys));

@@ -53,6 +53,12 @@ struct PatternDev {
     // refactor writes only these entries of the fp64 block; the dense kernel
     // reads every other entry as 0 in its first panel step.
     const unsigned* tail_mask;
+    // Column records of the refactorization, three 16-byte words per claim
+    // index idx (column k = col_order[idx]): {k, cp[k], column length,
+    // diagonal offset}, {first input entry a_ptr[k], a_ptr[k + 1],
+    // dependencies before the dense block, bwd_pos[k]}, {rel_ptr[k] low and
+    // high words, a_diag[k], 0}.
+    const int4* crec;
     const int* a_diag;       // [n] slot offset of A(q_k, q_k) in column k, or -1
     const int* bwd_pos;      // [n] row -> index in bwd_order
     const int* fwd_ldesc;    // [nfwd_levels * 5] level descriptors (see host)

@@ -124,7 +124,9 @@ int check_opts(const lusp_batch_opts* o);
 void fill_params(SolveParams& prm, const lusp_batch_opts& o);
 int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, SmemPlan& plan);
 int kernel_occupancy(int prec, int inner, size_t smem, int block, int* occ);
-int refactor_occupancy(int prec, size_t smem, int block, int* occ);
+// spread: the spread-mode kernel (several CTAs per system, global-memory
+// synchronization) instead of the cluster kernel.
+int refactor_occupancy(int prec, size_t smem, int block, int* occ, bool spread = false);
 int refactor_block(const lusp_batch_opts& o, int nsys);
 // Solve-kernel CTA size and plan target for nsys systems when left at 0.
 void resolve_solve_shape(lusp_batch_opts& o, int nsys);

@@ -530,10 +530,23 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
     while (true) {
         const int idx = warp_claim(&ctl[0]);
         if (idx >= n) break;
-        const int k = P.col_order[idx];
-        const int c0 = P.cp[k], c1 = P.cp[k + 1];
-        const int d = P.dg[k] - c0, len = c1 - c0;
+        // The column's record (one broadcast load of three 16-byte words),
+        // then, all in flight together: this lane's first input entry, its
+        // first dependency, the destination of its first slot, and the input
+        // value.  The later entries (columns longer than a warp) load as
+        // they are reached.
+        const int4 ra = P.crec[3 * idx], rb = P.crec[3 * idx + 1], rc = P.crec[3 * idx + 2];
+        const int k = ra.x, c0 = ra.y, len = ra.z, d = ra.w;
+        const int a0 = rb.x, a1 = rb.y, dsp = rb.z, bpos = rb.w;
         const int* rows = P.ri + c0;
+        const int ta = a0 + lane;
+        const int adst = ta < a1 ? P.a_dst[ta] : -1;
+        const int asrc = ta < a1 ? P.a_src[ta] : -1;
+        const int aprev = (ta < a1 && ta > a0) ? P.a_dst[ta - 1] : -1;
+        const int jj0 = lane < dsp ? rows[lane] : 0;
+        const int2 bc0 = lane < dsp ? P.dep_bc[c0 + lane] : make_int2(0, 0);
+        const int sdst0 = lane < len ? P.slot_dst[c0 + lane] : -1;
+        const double av0 = asrc >= 0 ? S.a_val[asrc] : 0.0;
         double* x;
         if (len <= plan.wcap) {
             x = wx;
@@ -546,21 +559,20 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
             continue;
         }
         // A column of the dense trailing block applies only its dependencies
-        // before k0 here (they come first: rows ascending).
+        // before k0 here (they come first: rows ascending; dsp of them).
         const bool tailcol = k >= P.k0;
-        int dsp = d;
-        if (tailcol) {
-            int below = 0;
-            for (int t = lane; t < d; t += 32) below += rows[t] < P.k0;
-            dsp = __reduce_add_sync(0xffffffffu, below);
-        }
         for (int t = lane; t < len; t += 32) x[t] = 0.0;
         __syncwarp();
-        const int a0 = P.a_ptr[k], a1 = P.a_ptr[k + 1];
         // The factor of A + shift diag|A(i,i)|: the input's diagonal entry
         // (duplicates summed first) gains shift times its magnitude.
-        const int adg = prm.shift != 0.0 ? P.a_diag[k] : -1;
-        for (int t = a0 + lane; t < a1; t += 32) {
+        const int adg = prm.shift != 0.0 ? rc.z : -1;
+        if (ta < a1 && (ta == a0 || aprev != adst)) {
+            double s = av0;
+            for (int u = ta + 1; u < a1 && P.a_dst[u] == adst; u++) s = __dadd_rn(s, S.a_val[P.a_src[u]]);
+            if (adst == adg) s = __dadd_rn(s, __dmul_rn(prm.shift, fabs(s)));
+            x[adst] = s;
+        }
+        for (int t = a0 + 32 + lane; t < a1; t += 32) {
             const int dst = P.a_dst[t];
             if (t == a0 || P.a_dst[t - 1] != dst) {
                 double s = S.a_val[P.a_src[t]];
@@ -579,14 +591,15 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         // plan.scap gathered entries; their L values and relative slots are
         // copied to shared memory with all copies in flight together, then
         // applied.
-        long long roff = have_rel ? P.rel_ptr[k] : 0;   // rel index of dependency u0
+        // rel index of dependency u0
+        long long roff = have_rel ? (long long)(((unsigned long long)(unsigned)rc.y << 32) | (unsigned)rc.x) : 0;
         for (int u0 = 0; u0 < dsp;) {
             const int u = u0 + lane;
             int beg = 0, cnt = 0;
             bool rdy = true;
             if (u < dsp) {
-                const int jj = rows[u];
-                const int2 bc = P.dep_bc[c0 + u];
+                const int jj = u0 == 0 ? jj0 : rows[u];
+                const int2 bc = u0 == 0 ? bc0 : P.dep_bc[c0 + u];
                 beg = bc.x;
                 cnt = bc.y;
                 rdy = is_ready(ready, jj);
@@ -679,7 +692,25 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 const int o_t = __shfl_sync(0xffffffffu, excl, t);
                 const int vo_t = __shfl_sync(0xffffffffu, vexcl + vsh, t);
                 const double xj = x[u0 + t];
-                if (xj != 0.0) {
+                if (xj != 0.0 && c_t <= 32) {
+                    // A short dependency column: one entry per lane.
+                    if (lane < c_t) {
+                        const int s = (int)srel[sh + o_t + lane];
+                        const double l = ValTraits<VT>::load(sval + vo_t + lane);
+                        x[s] = __dsub_rn(x[s], __dmul_rn(l, xj));
+                    }
+                } else if (xj != 0.0 && c_t <= 64) {
+                    // Two entries per lane, both loaded before either store
+                    // (rows of one dependency are distinct).
+                    const bool h = lane + 32 < c_t;
+                    const int s0 = (int)srel[sh + o_t + lane];
+                    const int s1 = h ? (int)srel[sh + o_t + lane + 32] : s0;
+                    const double l0 = ValTraits<VT>::load(sval + vo_t + lane);
+                    const double l1 = h ? ValTraits<VT>::load(sval + vo_t + lane + 32) : 0.0;
+                    const double x0 = x[s0], x1 = x[s1];
+                    x[s0] = __dsub_rn(x0, __dmul_rn(l0, xj));
+                    if (h) x[s1] = __dsub_rn(x1, __dmul_rn(l1, xj));
+                } else if (xj != 0.0) {
                     // Rows of one dependency are distinct: four entries per
                     // lane are loaded before any is written back.
                     for (int e = lane; e < c_t; e += 128) {
@@ -714,7 +745,7 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 const double v = x[t];
                 if (t < dsp) {
                     maxu = fmax(maxu, fabs(v));
-                    uval[P.slot_dst[c0 + t]] = ValTraits<VT>::to(v);
+                    uval[t < 32 ? sdst0 : P.slot_dst[c0 + t]] = ValTraits<VT>::to(v);
                 } else {
                     W[(size_t)(rows[t] - P.k0) * P.tail_ld + (k - P.k0)] = v;
                 }
@@ -749,11 +780,11 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
             if (t > d) v = __ddiv_rn(v, piv);
             else maxu = fmax(maxu, fabs(v));
             const VT sv = ValTraits<VT>::to(v);
-            const int dst = P.slot_dst[slot];
+            const int dst = t < 32 ? sdst0 : P.slot_dst[slot];
             if (t < d) uval[dst] = sv;
             else if (t == d) {
                 udiag[k] = sv;
-                ((VT*)S.udiag_bwd)[P.bwd_pos[k]] = ValTraits<VT>::to(1.0 / piv);
+                ((VT*)S.udiag_bwd)[bpos] = ValTraits<VT>::to(1.0 / piv);
             } else {
                 lu[slot] = sv;
                 lval[dst] = sv;
@@ -1030,7 +1061,11 @@ __device__ __forceinline__ void sweep_barrier(int nthreads) {
     asm volatile("bar.sync 1, %0;\n" ::"r"(nthreads) : "memory");
 }
 
-template <typename VT, bool UPPER>
+// GY: y lives in global memory (large systems): levels of a few long rows
+// (64 entries or more on average) get several warps per row, and long rows
+// four partial sums per lane; with y in shared memory a lane keeps one sum
+// and a row at most one warp.
+template <typename VT, bool UPPER, bool GY>
 __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* lgl, const int* order, const int* rp,
                              const int* ci, const VT* val, const VT* dgo, double* y,
                              char* stage, int cap_e, int cap_r, double* part) {
@@ -1083,7 +1118,9 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
         const VT* dd = st ? (const VT*)(base + (size_t)CE * (4 + sizeof(VT))) : dgo;
         const int eb = st ? (d.z & ~3) : 0, rb = st ? (r0 & ~3) : 0;
         const int lgd = lgl[L];
-        if (lgd > 5) {
+        // Several warps per row only for rows long enough to pay for the two
+        // extra barriers.
+        if (GY && lgd > 5 && d.w - d.z >= 64 * nr) {
             // Threads per row: the largest power of two (32 .. 2^lgd) that
             // still gives every row of the level its own group in one pass.
             int gw = 32;
@@ -1123,7 +1160,15 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
             if (rbase + ((warp * 32) >> lg) >= r1) break;   // nothing left for this warp
             const int r = rbase + ((int)threadIdx.x >> lg);
             double acc = 0.0;
-            if (r < r1) acc = row_dot<VT>(vv, cc, y, rp[r] - eb + lig, rp[r + 1] - eb, g);
+            if (r < r1) {
+                if (GY) {
+                    acc = row_dot<VT>(vv, cc, y, rp[r] - eb + lig, rp[r + 1] - eb, g);
+                } else {
+                    const int pe = rp[r + 1] - eb;
+                    for (int e = rp[r] - eb + lig; e < pe; e += g)
+                        acc = fma(ValTraits<VT>::load(vv + e), y[cc[e]], acc);
+                }
+            }
             for (int o = g >> 1; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, g);
             if (r < r1 && lig == 0) {
                 const int i = order[r];
@@ -1225,16 +1270,25 @@ __device__ void cta_lu_apply_levels(const SysDev& S, const PatternDev& P, const 
     for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = rhs[i];
     __syncthreads();
     const long long t0 = clock64();
-    staged_sweep<VT, false>(P.nfwd_levels, sd.f_ld, sd.f_lg, sd.f_ord, sd.f_rp, P.lci, (const VT*)S.lval,
-                            nullptr, y, stage, plan.sc_ent, plan.sc_rows, part);
+    const bool gy = P.n > plan.ycap;
+    if (gy)
+        staged_sweep<VT, false, true>(P.nfwd_levels, sd.f_ld, sd.f_lg, sd.f_ord, sd.f_rp, P.lci, (const VT*)S.lval,
+                                      nullptr, y, stage, plan.sc_ent, plan.sc_rows, part);
+    else
+        staged_sweep<VT, false, false>(P.nfwd_levels, sd.f_ld, sd.f_lg, sd.f_ord, sd.f_rp, P.lci,
+                                       (const VT*)S.lval, nullptr, y, stage, plan.sc_ent, plan.sc_rows, part);
     const long long t1 = clock64();
     if (P.dtail > 0) {
         tail_forward<VT>(P, (const VT*)S.tail, y, S.stats);
         tail_backward<VT>(P, (const VT*)S.tail, y, S.stats);
     }
     const long long t2 = clock64();
-    staged_sweep<VT, true>(P.nbwd_levels, sd.b_ld, sd.b_lg, sd.b_ord, sd.b_rp, P.uci, (const VT*)S.uval,
-                           (const VT*)S.udiag_bwd, y, stage, plan.sc_ent, plan.sc_rows, part);
+    if (gy)
+        staged_sweep<VT, true, true>(P.nbwd_levels, sd.b_ld, sd.b_lg, sd.b_ord, sd.b_rp, P.uci, (const VT*)S.uval,
+                                     (const VT*)S.udiag_bwd, y, stage, plan.sc_ent, plan.sc_rows, part);
+    else
+        staged_sweep<VT, true, false>(P.nbwd_levels, sd.b_ld, sd.b_lg, sd.b_ord, sd.b_rp, P.uci, (const VT*)S.uval,
+                                      (const VT*)S.udiag_bwd, y, stage, plan.sc_ent, plan.sc_rows, part);
     if (threadIdx.x == 0) {
         S.stats->cyc_lsolve += t1 - t0;
         S.stats->cyc_tail += t2 - t1;
@@ -1432,11 +1486,23 @@ __device__ __forceinline__ double cta_dot(const double* a, const double* b, int 
 // values: fp64 (outer residual, direct-solve residual) and, when the inner
 // products use it, fp32.  Ends with a CTA barrier.
 __device__ void build_sell_values(const SysDev& S, const PatternDev& P, bool f32) {
-    for (int t = threadIdx.x; t < P.sell_total; t += blockDim.x) {
-        const int s = P.sell_src[t];
-        const double v = s >= 0 ? S.a_val[s] : 0.0;
-        S.sell64[t] = v;
-        if (f32) S.sell32[t] = (float)v;
+    const int total = P.sell_total, nt = blockDim.x;
+    // Four entries per thread in flight (the value reads are gathers).
+    for (int t0 = threadIdx.x; t0 < total; t0 += 4 * nt) {
+        int src[4];
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) src[q] = t0 + q * nt < total ? P.sell_src[t0 + q * nt] : -1;
+#pragma unroll
+        for (int q = 0; q < 4; q++) v[q] = src[q] >= 0 ? S.a_val[src[q]] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int t = t0 + q * nt;
+            if (t < total) {
+                S.sell64[t] = v[q];
+                if (f32) S.sell32[t] = (float)v[q];
+            }
+        }
     }
     __syncthreads();
 }
