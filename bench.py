@@ -426,15 +426,26 @@ def suite_large(torch, api, mna, oracle, stream, flush, lib, spmv_reps=20, solve
     return out
 
 
-def suite_serving(torch, api, mna, oracle, stream):
-    """Poisson request stream over pattern classes through the serving loop:
-    90% fresh values on a cached pattern, 10% a new pattern, 5% ill-conditioned
-    (one subcircuit's conductances scaled to 1e-14); p50/p99 latency and
-    throughput vs plain per-request fp64 GPU solves."""
+def _pct(v, q):
+    return float(np.percentile(v, q)) if len(v) else None
+
+
+def suite_serving(torch, api, mna, oracle, stream, nreq=2000, rates=(2000.0, 2000.0, 2000.0, 10000.0),
+                  diag=None):
+    """Config 4: a Poisson refactor+solve request stream through the serving
+    loop over 64 pattern classes (n log-uniform in [113, 40000]; analog,
+    power-grid and supply-net generators in turn): 90% fresh values on a
+    cached pattern, 10% a new pattern (host analysis), 5% of the cached ones
+    ill-conditioned (a subcircuit's conductances scaled to 1e-14, a node held
+    only by gmin); HBM admission budget 150 GB.  Each rate runs its own
+    request set; throughput and p50/p99 latency overall and separately for
+    cached and new-pattern requests, beside plain per-request fp64 GPU
+    solves.  diag: optional path for per-request timings (JSON)."""
     rng = np.random.default_rng(42)
-    sizes = np.exp(rng.uniform(np.log(113), np.log(8000), 16)).astype(int)
-    classes = [mna.analog(int(n), 700 + i) for i, n in enumerate(sizes)]
-    nreq = 400
+    specs = mna.serving_classes(64)
+    t0 = time.perf_counter()
+    classes = [mna.serving_class(k, n, 700 + i) for i, (k, n) in enumerate(specs)]
+    gen_s = time.perf_counter() - t0
     new_id = [0]
 
     def make_requests(salt):
@@ -442,65 +453,87 @@ def suite_serving(torch, api, mna, oracle, stream):
         for r in range(nreq):
             u = rng.random()
             if u < 0.10:
-                m = mna.analog(int(rng.choice(sizes)), 5000 + new_id[0])
+                kind, n = specs[int(rng.integers(len(specs)))]
+                m = mna.serving_class(kind, n, 5000 + new_id[0])
                 new_id[0] += 1
-                v = m.Ax
+                reqs.append((m, m.Ax, True, False))
             else:
                 m = classes[int(rng.integers(len(classes)))]
-                v = m.perturbed(1, seed=salt + r)[0]
-                if rng.random() < 0.05:
-                    v = mna.ill_conditioned(m, seed=salt + r)
-            reqs.append((m, v))
+                ill = rng.random() < 0.05
+                v = mna.ill_conditioned(m, seed=salt + r) if ill else m.perturbed(1, seed=salt + r)[0]
+                reqs.append((m, v, False, ill))
         return reqs
-    out = {"workload": f"{nreq} requests over 16 analog pattern classes (n log-uniform [113, 8000]); 10% new "
-                       "patterns, 5% ill-conditioned; Poisson arrivals"}
-    S = api.Server(max_batch=64, streams=3, arena_gb=2.0, staging_mb=256)
-    for m in classes:            # warm the pattern cache (the classes are known ahead)
-        S.poll(S.submit(m.n, m.Ap, m.Ai, m.Ax, m.b), 120000)
-    # Untimed warm-up burst with the same mix (one-time costs of a fresh
-    # process and box: the first mixed launches, ladder launches, new-pattern
-    # analyses), its own values and new patterns.
-    warm = make_requests(1)
-    for i in [S.submit(m.n, m.Ap, m.Ai, v, m.b) for m, v in warm[:200]]:
-        S.poll(i, 300000)
-    for rate in (2000.0, 10000.0):
-        reqs = make_requests(int(rate))      # fresh values and fresh new patterns per rate
+
+    threads = max(4, (os.cpu_count() or 8) - 4)
+    out = {"workload": f"{nreq} requests per run over 64 pattern classes (n log-uniform [113, 40000]: analog, "
+                       "power-grid and supply-net generators); 10% new patterns, 5% of the cached ones "
+                       "ill-conditioned; Poisson arrivals; HBM budget 150 GB",
+           "class_generation_s": gen_s, "analysis_threads": threads}
+    S = api.Server(max_batch=64, streams=3, arena_gb=4.0, staging_mb=512, hbm_budget_gb=150.0,
+                   analysis_threads=threads)
+    t0 = time.perf_counter()
+    for i in [S.submit(m.n, m.Ap, m.Ai, m.Ax, m.b) for m in classes]:   # the classes are known ahead
+        S.poll(i, 600000)
+    out["class_analysis_s"] = time.perf_counter() - t0
+    # Untimed warm-up with the same mix (its own values and new patterns).
+    warm = make_requests(1)[:400]
+    for i in [S.submit(m.n, m.Ap, m.Ai, v, m.b) for m, v, _, _ in warm]:
+        S.poll(i, 600000)
+    runs, records = [], []
+    for ri, rate in enumerate(rates):
+        reqs = make_requests(1000 * (ri + 2))
         gaps = rng.exponential(1.0 / rate, nreq)
-        ids = []
+        ids, tsub = [], []
         t0 = time.perf_counter()
         tnext = t0
-        for (m, v), g in zip(reqs, gaps):
+        for (m, v, _, _), g in zip(reqs, gaps):
             tnext += g
             while time.perf_counter() < tnext:
                 pass
+            tsub.append(time.perf_counter() - t0)
             ids.append(S.submit(m.n, m.Ap, m.Ai, v, m.b))
-        res = [S.poll(i, 300000) for i in ids]
-        span = time.perf_counter() - t0
-        lat = [r[1]["latency_ms"] for r in res]
+        res = [S.poll(i, 600000) for i in ids]
+        done = np.array([ts + r[1]["latency_ms"] / 1000.0 for ts, r in zip(tsub, res)])
+        lat = np.array([r[1]["latency_ms"] for r in res])
+        new = np.array([q[2] for q in reqs])
+        hit = ~new
         ok = sum(int(r[1]["rc"] == 0) for r in res)
-        esc = sum(int(r[1]["escalated"]) for r in res)
         acc, chk = 0, 0
-        for (m, v), r in list(zip(reqs, res))[:: max(1, nreq // 40)]:
+        for (m, v, _, _), r in list(zip(reqs, res))[:: max(1, nreq // 40)]:
             ref = oracle.ref_cpu_solve(m.n, m.Ap, m.Ai, v, api.colamd(m.n, m.Ap, m.Ai), m.b)
             if ref is None:
                 continue
             chk += 1
             acc += int(np.linalg.norm(r[0] - ref) / np.linalg.norm(ref) <= 1e-6)
-        out[f"rate_{int(rate)}_per_s"] = {"p50_ms": float(np.percentile(lat, 50)),
-                                          "p99_ms": float(np.percentile(lat, 99)),
-                                          "throughput_per_s": nreq / span, "completed_ok": ok,
-                                          "escalated": esc, "accepted_in_sample": f"{acc}/{chk}",
-                                          "mean_batch": float(np.mean([r[1]["batch_size"] for r in res]))}
+        run = {"offered_per_s": rate, "arrival_window_s": float(tsub[-1]),
+               "throughput_per_s": nreq / float(done.max()),
+               "cached": {"count": int(hit.sum()), "throughput_per_s": int(hit.sum()) / float(done[hit].max()),
+                          "p50_ms": _pct(lat[hit], 50), "p99_ms": _pct(lat[hit], 99)},
+               "new_pattern": {"count": int(new.sum()), "p50_ms": _pct(lat[new], 50), "p99_ms": _pct(lat[new], 99),
+                               "last_done_s": float(done[new].max()) if new.any() else None},
+               "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "completed_ok": ok,
+               "escalated": sum(int(r[1]["escalated"]) for r in res),
+               "accepted_in_sample": f"{acc}/{chk}",
+               "mean_batch": float(np.mean([r[1]["batch_size"] for r in res]))}
+        runs.append(run)
+        records.append([{"t_submit": ts, "latency_ms": r[1]["latency_ms"], "queue_ms": r[1]["queue_ms"],
+                         "device_ms": r[1]["device_ms"], "batch": r[1]["batch_size"], "new": bool(q[2]),
+                         "ill": bool(q[3]), "n": int(q[0].n), "escalated": r[1]["escalated"]}
+                        for ts, r, q in zip(tsub, res, reqs)])
+    out["runs"] = runs
+    same = [r["cached"]["throughput_per_s"] for r, rate in zip(runs, rates) if rate == rates[0]]
+    out["cached_throughput_spread"] = (max(same) - min(same)) / float(np.mean(same)) if same else None
     out["server_stats"] = S.stats()
     S.close()
-    # Plain per-request fp64 GPU solves of the same requests (patterns analysed beforehand).
-    pat_cache = {}
+    # Plain per-request fp64 GPU solves of cached-pattern requests (patterns
+    # analysed beforehand, one launch each, copies included).
     times = []
-    for m, v in reqs[:100]:
-        key = id(m)
-        if key not in pat_cache:
-            pat_cache[key] = api.Pattern.from_matrix(m)
-        B = api.Batch([pat_cache[key]], prec=api.FP64)
+    sample = [q for q in make_requests(99)[:300] if not q[2]][:200]
+    pat_cache = {}
+    for m, v, _, _ in sample:
+        if id(m) not in pat_cache:
+            pat_cache[id(m)] = api.Pattern.from_matrix(m)
+        B = api.Batch([pat_cache[id(m)]], prec=api.FP64)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         B.upload([v], [m.b], stream=stream)
@@ -511,7 +544,9 @@ def suite_serving(torch, api, mna, oracle, stream):
         times.append(a.elapsed_time(b))
         B.close()
     out["fp64_per_request"] = {"mean_ms": statistics.mean(times), "per_s": 1000.0 / statistics.mean(times),
-                               "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99))}
+                               "p50_ms": _pct(times, 50), "p99_ms": _pct(times, 99)}
+    if diag:
+        Path(diag).write_text(json.dumps(records))
     return out
 
 
@@ -524,7 +559,7 @@ def run_suite(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     parts = {"uneven": lambda: suite_uneven(torch, api, mna, oracle, stream, flush),
              "large": lambda: suite_large(torch, api, mna, oracle, stream, flush, L.load()),
-             "serving": lambda: suite_serving(torch, api, mna, oracle, stream)}
+             "serving": lambda: suite_serving(torch, api, mna, oracle, stream, diag=args.diag or None)}
     for name in args.suite.split(","):
         print(json.dumps({"suite": name, **parts[name]()}), flush=True)
 
@@ -604,6 +639,7 @@ def main():
                     help="skip the other workloads' keys (configs 0, 2, 3) of the default line")
     ap.add_argument("--suite", default="", help="comma list of uneven,large,serving: the other "
                     "workloads, one JSON line each, instead of the default run")
+    ap.add_argument("--diag", default="", help="--suite serving: write per-request timings to this file")
     args = ap.parse_args()
     if args.suite:
         run_suite(args)

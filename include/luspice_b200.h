@@ -282,7 +282,9 @@ typedef struct {
 } lusp_server_opts;
 
 typedef struct {
-    int rc;                        /* LUSP_OK, LUSP_ESINGULAR (analysis), LUSP_EARG */
+    int rc;                        /* LUSP_OK, LUSP_ESINGULAR (analysis), LUSP_EARG,
+                                      LUSP_EALLOC (refused: larger than a stream arena or
+                                      than the pattern cache's HBM budget) */
     int status;                    /* LUSP_ST_* of the final attempt */
     double latency_ms;             /* submit -> result available */
     double queue_ms;               /* submit -> launch */
@@ -296,6 +298,14 @@ typedef struct {
     long long submitted, completed, escalated, cache_hits, cache_misses, evictions, launches;
     long long patterns_resident, max_batch_seen;
     double pattern_gb;
+    long long refused;             /* patterns refused by admission: larger than the
+                                      pattern cache's share of hbm_budget_gb (their
+                                      requests complete with LUSP_EALLOC and
+                                      LUSP_ST_CAPACITY) */
+    long long promoted;            /* times a pattern started its requests on the fp64
+                                      factor + GMRES-IR path after two escalations in a
+                                      row (one mixed trial every 16 requests) */
+    long long fp64_starts;         /* requests started on that path */
 } lusp_server_stats;
 
 void lusp_server_opts_default(lusp_server_opts *o);

@@ -63,7 +63,8 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("escalated", C.c_longlong),
                 ("cache_hits", C.c_longlong), ("cache_misses", C.c_longlong), ("evictions", C.c_longlong),
                 ("launches", C.c_longlong), ("patterns_resident", C.c_longlong),
-                ("max_batch_seen", C.c_longlong), ("pattern_gb", C.c_double)]
+                ("max_batch_seen", C.c_longlong), ("pattern_gb", C.c_double), ("refused", C.c_longlong),
+                ("promoted", C.c_longlong), ("fp64_starts", C.c_longlong)]
 
 
 class Coo(C.Structure):

@@ -51,7 +51,23 @@ struct PatternEntry {
     long long last_use = 0;
     bool own = false;              // pivots chosen for one request's values:
                                    // never matched by a lookup
+    // Escalation memory (a dynamic trial per pattern, not a condition
+    // estimate): after two mixed requests in a row escalated, new requests
+    // of the pattern start on the fp64 factor + GMRES-IR path, and every
+    // kTrialEvery-th tries the mixed path again; a trial that succeeds
+    // without escalation returns the pattern to the mixed path.
+    int esc_run = 0;
+    bool promoted = false;
+    int since_trial = 0;
 };
+constexpr int kTrialEvery = 16;
+
+// Requests are batched with others of their size class only, so a launch of
+// small systems never waits for a system hundreds of times larger.
+int size_class(int n) { return n < 2048 ? 0 : n < 12288 ? 1 : 2; }
+// Launch cap of the large class: few enough systems that each is spread
+// over several SMs (spread mode) instead of one 2-SM cluster.
+constexpr int kLargeBatch = 8;
 
 // MODE_FP64: the plain fp64 path (direct solve), for a server created in
 // fp64; MODE_FP64_IR: a failed mixed system once more with an fp64 factor
@@ -68,6 +84,8 @@ struct Request {
     bool cache_hit = false;
     bool escalated = false;
     bool repivoted = false;        // analysed again with its own values
+    bool trial = false;            // a mixed trial of a promoted pattern
+    bool learned = false;          // its mixed attempt has updated the pattern's memory
     bool done = false;
     Clock::time_point t_submit, t_launch, t_done;
     lusp_serve_result res{};
@@ -195,7 +213,15 @@ void ServerObj::analysis_loop() {
         const int rc = pattern_build(pe->n, pe->Ap.data(), pe->Ai.data(), pe->Ax.data(), nullptr, &P);
         {
             std::lock_guard<std::mutex> lk(mu);
-            if (rc == LUSP_OK) {
+            if (rc == LUSP_OK && P->bytes > pattern_budget) {
+                // Admission: a pattern larger than the cache's whole share
+                // of the HBM budget is refused (its requests complete with
+                // LUSP_EALLOC); its device copy leaves when nothing runs.
+                to_free.push_back(P);
+                pe->state = PAT_FAILED;
+                pe->fail_rc = LUSP_EALLOC;
+                stats.refused++;
+            } else if (rc == LUSP_OK) {
                 pe->pat = P;
                 pe->state = PAT_READY;
                 pattern_bytes += P->bytes;
@@ -262,7 +288,7 @@ bool ServerObj::try_launch(Flight& f) {
         Request* r = *it;
         if (r->pe->state == PAT_FAILED) {
             r->res.rc = r->pe->fail_rc;
-            r->res.status = LUSP_ST_SINGULAR;
+            r->res.status = r->pe->fail_rc == LUSP_EALLOC ? LUSP_ST_CAPACITY : LUSP_ST_SINGULAR;
             r->t_done = Clock::now();
             r->res.latency_ms = ms_since(r->t_submit, r->t_done);
             r->done = true;
@@ -274,9 +300,13 @@ bool ServerObj::try_launch(Flight& f) {
             ++it;
         }
     }
-    int mode = -1;
+    int mode = -1, cls = -1;
     for (Request* r : queue)
-        if (r->pe->state == PAT_READY) { mode = r->mode; break; }
+        if (r->pe->state == PAT_READY) {
+            mode = r->mode;
+            cls = size_class(r->n);
+            break;
+        }
     if (mode < 0) return false;
     lusp_batch_opts o = opts.solver;
     o.prec = fp64_mode(mode) ? LUSP_FP64 : LUSP_MIXED;
@@ -286,10 +316,10 @@ bool ServerObj::try_launch(Flight& f) {
     std::vector<Request*> pick;
     std::vector<PatternObj*> pats;
     size_t up_bytes = 0, down_bytes = 0, priv = 0;
-    const int maxb = std::max(1, opts.max_batch);
+    const int maxb = std::max(1, cls == 2 ? std::min(opts.max_batch, kLargeBatch) : opts.max_batch);
     for (Request* r : queue) {
         if ((int)pick.size() >= maxb) break;
-        if (r->pe->state != PAT_READY || r->mode != mode) continue;
+        if (r->pe->state != PAT_READY || r->mode != mode || size_class(r->n) != cls) continue;
         const StaticPattern& S = r->pe->pat->S;
         const size_t up = (r->vals.size() + r->rhs.size()) * 8;
         const size_t down = (size_t)S.n * 8 + sizeof(SysStats);
@@ -326,7 +356,7 @@ bool ServerObj::try_launch(Flight& f) {
     LaunchArgs la;
     LadderPlan lp;
     int grid = 0;
-    size_t nval = 0, nvec = 0, spill = 0;
+    size_t nval = 0, nvec = 0, spill = 0, syncb = 0;
     const lusp_batch_opts o_req = o;
     while (true) {
         const int nsp = (int)pick.size();
@@ -349,8 +379,8 @@ bool ServerObj::try_launch(Flight& f) {
         if (kernel_occupancy(o.prec, o.inner_prec, plan.bytes, o.block_threads, &occ) != LUSP_OK || occ < 1)
             return false;
         grid = std::min(nsp, occ * sm_count());
-        o.refactor_spread = -1;   // the arenas hold no per-system sync areas
         if (refactor_setup(pats, o, nsp, la) != LUSP_OK) return false;
+        syncb = la.rspread.group > 0 ? al((size_t)nsp * la.rspread.stride * sizeof(unsigned)) : 0;
         spill = spill_bytes(la.rgrid, la.rblock, cm, la.rplan);
         // Device-side escalation of the mixed path: a few ladder slots with
         // room for the largest systems of the launch.
@@ -369,7 +399,7 @@ bool ServerObj::try_launch(Flight& f) {
             if (ladder_setup(pats, lo, cap, la, lp, pool) != LUSP_OK) return false;
         }
         const size_t total = al(nval * 8) + 2 * al(nvec * 8) + privs + spill + al(sizeof(SysStats) * nsp) +
-                             al(sizeof(SysDev) * nsp) + 256 + lp.bytes;
+                             al(sizeof(SysDev) * nsp) + 256 + lp.bytes + syncb;
         if (total <= f.arena_bytes) break;
         if (nsp == 1) {
             Request* r = pick[0];
@@ -419,6 +449,9 @@ bool ServerObj::try_launch(Flight& f) {
     p += 256;
     char* d_ladder = p;
     p += lp.bytes;
+    // Spread mode: the systems' sync areas (zeroed by the launch).
+    if (syncb) la.rspread.sync = (unsigned*)p;
+    p += syncb;
     if ((size_t)(p - a) > f.arena_bytes) return false;
     ladder_bind(la, lp, d_ladder, d_queue);
     for (int i = 0; i < ns; i++) {
@@ -499,6 +532,23 @@ void ServerObj::complete(Flight& f) {
         const int hard = LUSP_ST_SINGULAR | LUSP_ST_STAGNATED | LUSP_ST_NOT_CONVERGED | LUSP_ST_NONFINITE;
         const bool fp64_failed = (s.rung > 0 || r->mode == MODE_FP64_IR) &&
                                  ((s.status & hard) != 0 || !(s.nres > 0 && s.res[s.nres - 1] <= opts.solver.rtol));
+        // The outcome of a request's mixed attempt updates its pattern's
+        // escalation memory (r->pe is still the shared pattern here: only an
+        // fp64 attempt re-pivots).
+        if (!r->learned && !fp64_mode(r->mode) && opts.escalate) {
+            r->learned = true;
+            PatternEntry* pe = r->pe;
+            if (s.rung > 0 || failed) {
+                if (++pe->esc_run >= 2 && !pe->promoted) {
+                    pe->promoted = true;
+                    pe->since_trial = 0;
+                    stats.promoted++;
+                }
+            } else {
+                pe->esc_run = 0;
+                if (r->trial && pe->promoted) pe->promoted = false;
+            }
+        }
         if (fp64_failed && !r->repivoted && opts.escalate) {
             auto npe = std::make_unique<PatternEntry>();
             npe->key = r->pe->key;
@@ -674,6 +724,17 @@ long long lusp_serve_submit(lusp_server* s, int n, const int* Ap, const int* Ai,
         if (pe) {
             r->cache_hit = true;
             S->stats.cache_hits++;
+            // A pattern whose mixed requests keep escalating starts on the
+            // fp64 factor + GMRES-IR path, with a mixed trial now and then.
+            if (pe->promoted && !lusp::fp64_mode(r->mode)) {
+                if (++pe->since_trial >= lusp::kTrialEvery) {
+                    pe->since_trial = 0;
+                    r->trial = true;
+                } else {
+                    r->mode = lusp::MODE_FP64_IR;
+                    S->stats.fp64_starts++;
+                }
+            }
         } else {
             auto npe = std::make_unique<lusp::PatternEntry>();
             npe->key = key;

@@ -315,6 +315,34 @@ def ill_conditioned(m: MNAMatrix, seed: int, width: int = 8, scale: float = 1e-1
     return m.values(fac)
 
 
+SERVING_KINDS = ("analog", "grid", "supply")
+
+
+def serving_class(kind: str, n: int, seed: int) -> MNAMatrix:
+    """One pattern class of the serving workload, about n unknowns: "analog"
+    (the n = 989 generator at size n), "grid" (a power-grid mesh of about n
+    nodes with about n / 225 pads) or "supply" (the analog netlist with supply nets,
+    the n = 40,000 generator at size n)."""
+    if kind == "analog":
+        return analog(int(n), seed)
+    if kind == "grid":
+        pads = 3 * max(1, int(n) // 675)      # a 3 x (pads / 3) lattice of pads
+        rows = max(2, int(np.sqrt(max(4, int(n) - pads))))
+        cols = max(2, (int(n) - pads) // rows)
+        return power_grid(rows, cols, pads, seed)
+    if kind == "supply":
+        return large_circuit(max(int(n), 200), seed)
+    raise ValueError(kind)
+
+
+def serving_classes(count: int = 64, lo: int = 113, hi: int = 40000, seed: int = 42) -> list[tuple[str, int]]:
+    """(kind, n) of the serving workload's pattern classes: n log-uniform in
+    [lo, hi], the three generators in turn."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(int)
+    return [(SERVING_KINDS[i % 3], int(n)) for i, n in enumerate(ns)]
+
+
 def batch_sizes(count: int = 512, lo: int = 100, hi: int = 5000, seed: int = 42) -> np.ndarray:
     """Matrix sizes of the uneven batch: n ~ U[lo, hi] from the base seed."""
     return np.random.default_rng(seed).integers(lo, hi + 1, count)

@@ -204,3 +204,75 @@ def test_lru_eviction_and_reanalysis(gpu):
     assert r["rc"] == 0 and not r["cache_hit"]
     assert rel_err(x, oracle_solution(m, v)) <= TOL_REL
     S.close()
+
+
+def test_admission_refuses_pattern_above_budget(gpu):
+    """HBM admission: with a pattern budget of a few MB beside the arena, a
+    pattern whose device layout alone exceeds it (the n = 4050 power grid,
+    ~14 MB) is refused with LUSP_EALLOC / CAPACITY, while small patterns
+    submitted before and after it are served."""
+    small = [mna.analog(300, 80 + i) for i in range(4)]
+    big = mna.power_grid()
+    arena = 0.25
+    S = api.Server(max_batch=4, streams=1, arena_gb=arena, staging_mb=64, hbm_budget_gb=arena + 0.002)
+    ids = [S.submit(m.n, m.Ap, m.Ai, m.Ax, m.b) for m in small[:2]]
+    ib = S.submit(big.n, big.Ap, big.Ai, big.Ax, big.b)
+    ids += [S.submit(m.n, m.Ap, m.Ai, m.Ax, m.b) for m in small[2:]]
+    xb, rb = S.poll(ib, 120000)
+    assert rb["rc"] == 2 and rb["status"] & api.ST_CAPACITY, rb   # LUSP_EALLOC
+    for m, i in zip(small, ids):
+        x, r = S.poll(i, 120000)
+        assert r["rc"] == 0, r
+        assert rel_err(x, oracle_solution(m, m.Ax)) <= TOL_REL
+    st = S.stats()
+    assert st["refused"] == 1 and st["pattern_gb"] <= 0.002 + 1e-9, st
+    S.close()
+
+
+def test_pattern_escalation_memory(gpu):
+    """A pattern whose mixed requests keep escalating (supply-net values over
+    15 decades, pivots frozen on the nominal values: fp32 inner products
+    stagnate) starts its later requests on the fp64 factor + GMRES-IR path
+    after two escalations in a row, with a mixed trial every 16th request.
+    The server's counters equal a replay of that rule over the observed
+    outcomes, the path is taken at least once, and every answer is the fp64
+    oracle's."""
+    m = mna.serving_class("supply", 1748, 726)
+    vals = m.perturbed(24, seed=5)
+    S = api.Server(max_batch=4, streams=1, arena_gb=0.5, staging_mb=32)
+    x0, r0 = S.poll(S.submit(m.n, m.Ap, m.Ai, m.Ax, m.b), 120000)   # pivots from the nominal values
+    assert r0["rc"] == 0
+    res = []
+    for v in vals:
+        x, r = S.poll(S.submit(m.n, m.Ap, m.Ai, v, m.b), 120000)
+        assert r["rc"] == 0, r
+        res.append((x, r))
+    st = S.stats()
+    S.close()
+    # Replay: the nominal request first, then the 24 in order.
+    outcomes = [bool(r0["escalated"])] + [bool(r["escalated"]) for _, r in res]
+    run, promoted, since, n_prom, n_fp64 = 0, False, 0, 0, 0
+    for i, esc in enumerate(outcomes):
+        trial = False
+        if promoted and i > 0:
+            since += 1
+            if since >= 16:
+                since, trial = 0, True
+            else:
+                n_fp64 += 1
+                assert not esc, f"request {i} started on the fp64 path but escalated"
+                continue
+        if esc:
+            run += 1
+            if run >= 2 and not promoted:
+                promoted, since, n_prom = True, 0, n_prom + 1
+        else:
+            run = 0
+            if trial and promoted:
+                promoted = False
+    assert n_prom >= 1, outcomes
+    assert st["promoted"] == n_prom and st["fp64_starts"] == n_fp64, (st, outcomes)
+    from luspice_b200.api import Pattern
+    _, q = Pattern.from_matrix(m).perm()
+    for (x, r), v in zip(res, vals):
+        assert rel_err(x, oracle_solution(m, v, q=q)) <= TOL_REL, r
