@@ -430,8 +430,8 @@ def _pct(v, q):
     return float(np.percentile(v, q)) if len(v) else None
 
 
-def suite_serving(torch, api, mna, oracle, stream, nreq=2000, rates=(2000.0, 2000.0, 2000.0, 10000.0),
-                  diag=None):
+def suite_serving(torch, api, mna, oracle, stream, nreq=2000,
+                  rates=(250.0, 250.0, 250.0, 500.0, 1000.0, 2000.0, 2000.0, 2000.0), diag=None):
     """Config 4: a Poisson refactor+solve request stream through the serving
     loop over 64 pattern classes (n log-uniform in [113, 40000]; analog,
     power-grid and supply-net generators in turn): 90% fresh values on a
@@ -496,6 +496,7 @@ def suite_serving(torch, api, mna, oracle, stream, nreq=2000, rates=(2000.0, 200
         done = np.array([ts + r[1]["latency_ms"] / 1000.0 for ts, r in zip(tsub, res)])
         lat = np.array([r[1]["latency_ms"] for r in res])
         new = np.array([q[2] for q in reqs])
+        nn = np.array([q[0].n for q in reqs])
         hit = ~new
         ok = sum(int(r[1]["rc"] == 0) for r in res)
         acc, chk = 0, 0
@@ -509,6 +510,11 @@ def suite_serving(torch, api, mna, oracle, stream, nreq=2000, rates=(2000.0, 200
                "throughput_per_s": nreq / float(done.max()),
                "cached": {"count": int(hit.sum()), "throughput_per_s": int(hit.sum()) / float(done[hit].max()),
                           "p50_ms": _pct(lat[hit], 50), "p99_ms": _pct(lat[hit], 99)},
+               "by_size": {name: {"count": int(sel.sum()), "p50_ms": _pct(lat[sel], 50), "p99_ms": _pct(lat[sel], 99),
+                                  "throughput_per_s": int(sel.sum()) / float(done[sel].max()) if sel.any() else None}
+                           for name, sel in (("n<2048", hit & (nn < 2048)),
+                                             ("2048<=n<12288", hit & (nn >= 2048) & (nn < 12288)),
+                                             ("n>=12288", hit & (nn >= 12288)))},
                "new_pattern": {"count": int(new.sum()), "p50_ms": _pct(lat[new], 50), "p99_ms": _pct(lat[new], 99),
                                "last_done_s": float(done[new].max()) if new.any() else None},
                "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "completed_ok": ok,
@@ -521,8 +527,12 @@ def suite_serving(torch, api, mna, oracle, stream, nreq=2000, rates=(2000.0, 200
                          "ill": bool(q[3]), "n": int(q[0].n), "escalated": r[1]["escalated"]}
                         for ts, r, q in zip(tsub, res, reqs)])
     out["runs"] = runs
-    same = [r["cached"]["throughput_per_s"] for r, rate in zip(runs, rates) if rate == rates[0]]
-    out["cached_throughput_spread"] = (max(same) - min(same)) / float(np.mean(same)) if same else None
+    # Agreement of back-to-back runs at the same offered rate.
+    out["throughput_spread"] = {}
+    for rate in sorted(set(rates)):
+        same = [r["throughput_per_s"] for r, rt in zip(runs, rates) if rt == rate]
+        if len(same) > 1:
+            out["throughput_spread"][str(int(rate))] = (max(same) - min(same)) / float(np.mean(same))
     out["server_stats"] = S.stats()
     S.close()
     # Plain per-request fp64 GPU solves of cached-pattern requests (patterns

@@ -99,6 +99,7 @@ struct Flight {
     char* stage = nullptr;          // pinned: [values | rhs] up, [x | stats] down
     size_t stage_bytes = 0;
     bool busy = false;
+    int cls = -1;                   // size class of the launch in flight
     std::vector<Request*> reqs;
     std::vector<size_t> x_off;      // per request, doubles into the download x area
     size_t down_x = 0, down_stats = 0;
@@ -300,9 +301,15 @@ bool ServerObj::try_launch(Flight& f) {
             ++it;
         }
     }
+    // The oldest ready request sets the launch's mode and size class; large
+    // systems may hold all but one stream, so launches of small and medium
+    // systems never queue behind them.
+    int nlarge = 0;
+    for (const Flight& g : flights) nlarge += g.busy && g.cls == 2;
+    const bool allow_large = nlarge < std::max(1, (int)flights.size() - 1);
     int mode = -1, cls = -1;
     for (Request* r : queue)
-        if (r->pe->state == PAT_READY) {
+        if (r->pe->state == PAT_READY && (allow_large || size_class(r->n) != 2)) {
             mode = r->mode;
             cls = size_class(r->n);
             break;
@@ -498,6 +505,7 @@ bool ServerObj::try_launch(Flight& f) {
     // Hand the requests to the flight.
     f.reqs = pick;
     f.busy = true;
+    f.cls = cls;
     for (Request* r : pick) {
         r->t_launch = now;
         r->res.batch_size = ns;

