@@ -593,13 +593,18 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         // applied.
         // rel index of dependency u0
         long long roff = have_rel ? (long long)(((unsigned long long)(unsigned)rc.y << 32) | (unsigned)rc.x) : 0;
+        // Dependency metadata of the round starting at pf_u0, loaded while
+        // the previous round's copies and updates ran.
+        int pf_u0 = 0, pf_jj = jj0;
+        int2 pf_bc = bc0;
         for (int u0 = 0; u0 < dsp;) {
             const int u = u0 + lane;
             int beg = 0, cnt = 0;
             bool rdy = true;
             if (u < dsp) {
-                const int jj = u0 == 0 ? jj0 : rows[u];
-                const int2 bc = u0 == 0 ? bc0 : P.dep_bc[c0 + u];
+                const bool pre = u0 == pf_u0;
+                const int jj = pre ? pf_jj : rows[u];
+                const int2 bc = pre ? pf_bc : P.dep_bc[c0 + u];
                 beg = bc.x;
                 cnt = bc.y;
                 rdy = is_ready(ready, jj);
@@ -680,6 +685,12 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
                 const int o_t = __shfl_sync(0xffffffffu, vexcl, t);
                 for (int e = lane; e < p_t; e += 32) cp_async_16(sval + o_t + e * VPK, lu + a_t + e * VPK);
             }
+            // The next round's metadata, in flight with the copies.
+            pf_u0 = u0 + nfit;
+            if (pf_u0 + lane < dsp) {
+                pf_jj = __ldg(rows + pf_u0 + lane);
+                pf_bc = __ldg(P.dep_bc + c0 + pf_u0 + lane);
+            }
             cp_async_wait_all();
             __syncwarp();
             {
@@ -740,14 +751,27 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
             u0 += nfit;
         }
         if (tailcol) {
-            // U rows before k0 are final; the rest goes to the dense block.
-            for (int t = lane; t < len; t += 32) {
-                const double v = x[t];
-                if (t < dsp) {
-                    maxu = fmax(maxu, fabs(v));
-                    uval[t < 32 ? sdst0 : P.slot_dst[c0 + t]] = ValTraits<VT>::to(v);
-                } else {
-                    W[(size_t)(rows[t] - P.k0) * P.tail_ld + (k - P.k0)] = v;
+            // U rows before k0 are final; the rest goes to the dense block
+            // (destinations of four slots per lane loaded first).
+            for (int t0 = lane; t0 < len; t0 += 128) {
+                int dst[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int t = t0 + 32 * q;
+                    dst[q] = t >= len ? 0 : t < dsp ? (t < 32 ? sdst0 : __ldg(P.slot_dst + c0 + t))
+                                                    : __ldg(rows + t);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int t = t0 + 32 * q;
+                    if (t >= len) break;
+                    const double v = x[t];
+                    if (t < dsp) {
+                        maxu = fmax(maxu, fabs(v));
+                        uval[dst[q]] = ValTraits<VT>::to(v);
+                    } else {
+                        W[(size_t)(dst[q] - P.k0) * P.tail_ld + (k - P.k0)] = v;
+                    }
                 }
             }
             __syncwarp();
@@ -773,21 +797,32 @@ __device__ void refactor_phase(const SysDev& S, const SmemPlan& plan, char* smem
         if (ratio < prm.pivot_tol) bad |= ST_PIVOT_WEAK;
         // Each value is stored once where the solves read it (U rows, the
         // diagonal, L rows); the strict-L part also goes to the merged
-        // columns, which the later columns' gathers read.
-        for (int t = lane; t < len; t += 32) {
-            const int slot = c0 + t;
-            double v = x[t];
-            if (t > d) v = __ddiv_rn(v, piv);
-            else maxu = fmax(maxu, fabs(v));
-            const VT sv = ValTraits<VT>::to(v);
-            const int dst = t < 32 ? sdst0 : P.slot_dst[slot];
-            if (t < d) uval[dst] = sv;
-            else if (t == d) {
-                udiag[k] = sv;
-                ((VT*)S.udiag_bwd)[bpos] = ValTraits<VT>::to(1.0 / piv);
-            } else {
-                lu[slot] = sv;
-                lval[dst] = sv;
+        // columns, which the later columns' gathers read.  The destinations
+        // of four slots per lane are loaded before any of their stores (the
+        // loads could not move above the stores of an earlier slot).
+        for (int t0 = lane; t0 < len; t0 += 128) {
+            int dst[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int t = t0 + 32 * q;
+                dst[q] = t < len ? (t < 32 ? sdst0 : __ldg(P.slot_dst + c0 + t)) : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int t = t0 + 32 * q;
+                if (t >= len) break;
+                double v = x[t];
+                if (t > d) v = __ddiv_rn(v, piv);
+                else maxu = fmax(maxu, fabs(v));
+                const VT sv = ValTraits<VT>::to(v);
+                if (t < d) uval[dst[q]] = sv;
+                else if (t == d) {
+                    udiag[k] = sv;
+                    ((VT*)S.udiag_bwd)[bpos] = ValTraits<VT>::to(1.0 / piv);
+                } else {
+                    lu[c0 + t] = sv;
+                    lval[dst[q]] = sv;
+                }
             }
         }
         // Release: the column's values before its ready bit.
