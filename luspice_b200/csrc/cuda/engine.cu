@@ -390,8 +390,8 @@ int pattern_build(int n, const int* Ap, const int* Ai, const double* Ax, const i
     D.crec = (const int4*)(blk + off[idx++]);
     D.lev_max_ent = S.lev_max_ent;
     D.lev_max_rows = S.lev_max_rows;
-    D.nfwd_levels = S.nfwd_levels;
-    D.nbwd_levels = S.nbwd_levels;
+    D.nfwd_levels = S.nfwd_steps;   // the device walks the sweep steps
+    D.nbwd_levels = S.nbwd_steps;
     D.k0 = S.k0;
     D.dtail = S.dtail;
     D.tail_ld = tail_ld(S);
@@ -450,7 +450,7 @@ void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm,
     int nmax = 1, levmax = 1, entmax = 4, rowmax = 4;
     for (auto* p : pats) {
         nmax = std::max(nmax, p->S.n);
-        levmax = std::max(levmax, p->S.nfwd_levels + p->S.nbwd_levels);
+        levmax = std::max(levmax, p->S.nfwd_steps + p->S.nbwd_steps);
         entmax = std::max(entmax, p->S.lev_max_ent);
         rowmax = std::max(rowmax, p->S.lev_max_rows);
     }
@@ -554,9 +554,10 @@ void make_dense_plan(const std::vector<PatternObj*>& pats, int threads, SmemPlan
     const size_t budget = 227 * 1024;
     plan.bytes = fixed;
     if (dmax == 0) return;
-    // Panel [D][nb + 1] (padded rows) + U tile [nb][128] + nb column maxima
-    // + 4 cycle counters: the widest panel (32, 16, 8) that fits.
-    auto dneed = [&](int nb) { return fixed + 8 * ((size_t)dmax * (nb + 1) + (size_t)nb * 128 + nb + 4); };
+    // Panel [D][nb + 1] (padded rows) + U tile [nb][128] + per-warp column
+    // maxima [nb][32] + 4 cycle counters: the widest panel (32, 16, 8) that
+    // fits.
+    auto dneed = [&](int nb) { return fixed + 8 * ((size_t)dmax * (nb + 1) + (size_t)nb * 128 + (size_t)nb * 32 + 4); };
     int nb = 32;
     while (nb > 8 && dneed(nb) > budget) nb /= 2;
     plan.tnb = nb;

@@ -18,7 +18,7 @@ namespace lusp {
 struct PatternDev {
     int n, nnz_a, cap, max_col, nslices, sell_total;
     int nnz_l, nnz_u;        // strict L and strict U entries
-    int nfwd_levels, nbwd_levels;
+    int nfwd_levels, nbwd_levels;    // sweep steps (descriptors) of each sweep
     const int* cp;           // [n+1] merged column pointers
     const int* ri;           // [cap] row positions, ascending per column
     const int* dg;           // [n]   slot of the diagonal

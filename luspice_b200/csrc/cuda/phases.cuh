@@ -164,8 +164,11 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     double* pan = (double*)sm.uni;                                           // [D][ps]
     double* ut = pan + (size_t)D * ps;                                       // [nb][128]
-    unsigned long long* cmax = (unsigned long long*)(ut + (size_t)nb * 128); // [nb]
-    long long* ctr = (long long*)(cmax + nb);   // [4] stage cycles (thread 0)
+    // Per column of the panel, each warp's maximum |L| before scaling (the
+    // pivot statistics' denominator): a slot per warp, reduced after the
+    // panel, so the panel's column chain carries no atomics.
+    double* wmax = ut + (size_t)nb * 128;                                    // [nb][32]
+    long long* ctr = (long long*)(wmax + (size_t)nb * 32);   // [4] stage cycles (thread 0)
     if (tid == 0) {
         ctr[0] = ctr[1] = ctr[2] = 0;
         ctr[3] = clock64();
@@ -178,7 +181,6 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
             const int r = t / nb, c = t - r * nb;
             pan[r * ps + c] = c < w ? tail_entry(W, ld, mask, jb + r, jb + c, first) : 0.0;
         }
-        if (tid < nb) cmax[tid] = 0ull;
         __syncthreads();
         // Panel: unblocked elimination, a lane per row and a warp per 32
         // rows, so a row's multiplier and its update stay inside one warp:
@@ -212,14 +214,15 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
                 }
             }
             lm = warp_max(lm);
-            if (lane == 0 && lm > 0.0) atomicMax(&cmax[c], (unsigned long long)__double_as_longlong(lm));
+            if (lane == 0) wmax[c * 32 + warp] = lm;
             __syncthreads();
         }
         if (tid < w) {
             const int c = tid;
             const double piv = pan[c * ps + c];
             const double ap = fabs(piv);
-            const double amax = __longlong_as_double((long long)cmax[c]);
+            double amax = 0.0;
+            for (int q = 0; q < nw; q++) amax = fmax(amax, wmax[c * 32 + q]);
             if (!(ap > 0.0) || !isfinite(piv)) {
                 bad |= ST_SINGULAR;
                 atomicMin(&sm.ctl[2], k0 + jb + c);
@@ -1153,6 +1156,28 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
         const VT* dd = st ? (const VT*)(base + (size_t)CE * (4 + sizeof(VT))) : dgo;
         const int eb = st ? (d.z & ~3) : 0, rb = st ? (r0 & ~3) : 0;
         const int lgd = lgl[L];
+        if (lgd < 0) {
+            // A run of narrow levels: one warp, its rows in level order (a
+            // row's result is visible to the warp's next rows after the warp
+            // barrier), no CTA barrier until the run ends.
+            if (warp == 0) {
+                const int lane = threadIdx.x & 31;
+                for (int r = r0; r < r1; r++) {
+                    double acc = 0.0;
+                    const int pe = rp[r + 1] - eb;
+                    for (int e = rp[r] - eb + lane; e < pe; e += 32)
+                        acc = fma(ValTraits<VT>::load(vv + e), y[cc[e]], acc);
+                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+                    if (lane == 0) {
+                        const int i = order[r];
+                        if (UPPER) y[i] = (y[i] - acc) * ValTraits<VT>::load(dd + (r - rb));
+                        else y[i] = y[i] - acc;
+                    }
+                    __syncwarp();
+                }
+            }
+            continue;
+        }
         // Several warps per row only for rows long enough to pay for the two
         // extra barriers.
         if (GY && lgd > 5 && d.w - d.z >= 64 * nr) {

@@ -69,6 +69,8 @@ struct StaticPattern {
     std::vector<int> fwd_order, bwd_order;   // level-sorted row orders
     std::vector<int> fwd_lev, bwd_lev;
     int nfwd_levels = 0, nbwd_levels = 0;
+    int nfwd_steps = 0, nbwd_steps = 0;      // sweep steps (descriptors): levels,
+                                             // with runs of narrow levels merged
     std::vector<int> bwd_pos;                // row -> index in bwd_order
     // Level descriptors of the sweeps: nlev x {first row idx, end row idx,
     // first entry, end entry}, then nlev x log2(lanes per row).

@@ -8,6 +8,7 @@
 #include "lusp_host.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -449,42 +450,64 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
             for (int p = S.dg[k] + 1; p < S.cp[k + 1]; p++)
                 if (S.slot_dst[p] >= 0) S.slot_dst[p] = lmap[S.slot_dst[p]];
         }
-        // Per-level descriptors of both sweeps: first row, end row, first
-        // entry, end entry, and log2 of the lanes per row (the power of two
-        // at or above the level's mean row length, at most 512: above 32,
-        // several warps share a row when the level has few rows).
+        // Sweep steps of both sweeps, one descriptor each: first row, end
+        // row, first entry, end entry, and log2 of the lanes per row (the
+        // power of two at or above the step's mean row length, at most 512:
+        // above 32, several warps share a row when the step has few rows).
+        // A run of at least two consecutive levels of at most kChainRows
+        // rows each becomes one step processed by a single warp, its rows in
+        // level order (lanes log2 = -1): the warp finishes a row before it
+        // reads it, so the run costs no CTA barrier per level.  A run stops
+        // at kChainMaxRows rows or kChainMaxEnt entries (so it fits a stage).
+        constexpr int kChainRows = 3, kChainMaxRows = 128, kChainMaxEnt = 2048;
         auto level_desc = [](int nlev, const std::vector<int>& lev, const std::vector<int>& rp,
                              std::vector<int>& out) {
-            out.assign((size_t)nlev * 5, 0);
-            for (int l = 0; l < nlev; l++) {
+            std::vector<std::array<int, 5>> steps;
+            auto narrow = [&](int l) { return lev[l + 1] - lev[l] <= kChainRows; };
+            for (int l = 0; l < nlev;) {
+                if (narrow(l)) {
+                    int l2 = l;
+                    while (l2 < nlev && narrow(l2) && lev[l2 + 1] - lev[l] <= kChainMaxRows &&
+                           rp[lev[l2 + 1]] - rp[lev[l]] <= kChainMaxEnt)
+                        l2++;
+                    if (l2 - l >= 2) {
+                        steps.push_back({lev[l], lev[l2], rp[lev[l]], rp[lev[l2]], -1});
+                        l = l2;
+                        continue;
+                    }
+                }
                 const int r0 = lev[l], r1 = lev[l + 1];
                 const int e0 = rp[r0], e1 = rp[r1];
                 const int nr = std::max(1, r1 - r0);
                 const int mean = (e1 - e0 + nr - 1) / nr;
                 int lg = 0;
                 while ((1 << lg) < mean && lg < 9) lg++;
-                out[(size_t)l * 4 + 0] = r0;
-                out[(size_t)l * 4 + 1] = r1;
-                out[(size_t)l * 4 + 2] = e0;
-                out[(size_t)l * 4 + 3] = e1;
-                out[(size_t)nlev * 4 + l] = lg;
+                steps.push_back({r0, r1, e0, e1, lg});
+                l++;
             }
+            const int ns = (int)steps.size();
+            out.assign((size_t)ns * 5, 0);
+            for (int t = 0; t < ns; t++) {
+                for (int j = 0; j < 4; j++) out[(size_t)t * 4 + j] = steps[t][j];
+                out[(size_t)ns * 4 + t] = steps[t][4];
+            }
+            return ns;
         };
-        level_desc(S.nfwd_levels, S.fwd_lev, S.lrp, S.fwd_ldesc);
-        level_desc(S.nbwd_levels, S.bwd_lev, S.urp, S.bwd_ldesc);
+        S.nfwd_steps = level_desc(S.nfwd_levels, S.fwd_lev, S.lrp, S.fwd_ldesc);
+        S.nbwd_steps = level_desc(S.nbwd_levels, S.bwd_lev, S.urp, S.bwd_ldesc);
         // Position of each row in the backward order, and the widest level
         // of either sweep (entries, rows) for the shared-memory stages.
         S.bwd_pos.assign(n, 0);
         for (int idx = 0; idx < n; idx++) S.bwd_pos[S.bwd_order[idx]] = idx;
         S.lev_max_ent = 0;
         S.lev_max_rows = 0;
-        for (int l = 0; l < S.nfwd_levels; l++) {
-            S.lev_max_ent = std::max(S.lev_max_ent, S.lrp[S.fwd_lev[l + 1]] - S.lrp[S.fwd_lev[l]]);
-            S.lev_max_rows = std::max(S.lev_max_rows, S.fwd_lev[l + 1] - S.fwd_lev[l]);
-        }
-        for (int l = 0; l < S.nbwd_levels; l++) {
-            S.lev_max_ent = std::max(S.lev_max_ent, S.urp[S.bwd_lev[l + 1]] - S.urp[S.bwd_lev[l]]);
-            S.lev_max_rows = std::max(S.lev_max_rows, S.bwd_lev[l + 1] - S.bwd_lev[l]);
+        for (int pass = 0; pass < 2; pass++) {
+            const std::vector<int>& d = pass ? S.bwd_ldesc : S.fwd_ldesc;
+            const int ns = pass ? S.nbwd_steps : S.nfwd_steps;
+            for (int t = 0; t < ns; t++) {
+                S.lev_max_ent = std::max(S.lev_max_ent, d[(size_t)t * 4 + 3] - d[(size_t)t * 4 + 2]);
+                S.lev_max_rows = std::max(S.lev_max_rows, d[(size_t)t * 4 + 1] - d[(size_t)t * 4 + 0]);
+            }
         }
     }
 
