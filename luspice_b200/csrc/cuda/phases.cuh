@@ -1163,10 +1163,9 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
             if (warp == 0) {
                 const int lane = threadIdx.x & 31;
                 for (int r = r0; r < r1; r++) {
-                    double acc = 0.0;
-                    const int pe = rp[r + 1] - eb;
-                    for (int e = rp[r] - eb + lane; e < pe; e += 32)
-                        acc = fma(ValTraits<VT>::load(vv + e), y[cc[e]], acc);
+                    // Four loads per lane in flight (a run too large for a
+                    // stage reads global memory).
+                    double acc = row_dot<VT>(vv, cc, y, rp[r] - eb + lane, rp[r + 1] - eb, 32);
                     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
                     if (lane == 0) {
                         const int i = order[r];
