@@ -295,58 +295,15 @@ void build_static_pattern(int n, const int* Ap, const int* Ai, const int* q,
         ptr[n] = (int)dep.size();
         std::vector<int> visit(n);
         std::iota(visit.begin(), visit.end(), 0);
+        // The claim order of the refactorization is the level order (any
+        // topological order is safe: a warp waits only on columns claimed
+        // before its own).  Measured on B200 (n = 4050 grid, 48 warps per
+        // system): list schedules by longest remaining path, simulated on
+        // 24, 48 or 96 warps, and level order with the longest path first
+        // inside a level all refactor in the same time (2.22-2.28 ms); a
+        // longest-path-first order without regard to time, which hands a
+        // dependent chain to consecutive warps, takes 4.0 ms.
         levels_and_order(n, visit, ptr, dep, S.col_level, S.col_order, S.ncol_levels);
-        // Claim order of the refactorization: a topological order that takes,
-        // among the columns whose dependencies are all earlier in it, the one
-        // with the most estimated work on its longest path to the end (its
-        // "bottom level"; work of a column ~ a warp step per dependency plus
-        // one per 32 gathered entries).  Warps claim columns in this order and
-        // wait only on earlier ones, so any topological order is safe; the
-        // critical columns no longer queue behind same-level columns that
-        // nothing waits for.
-        {
-            std::vector<double> cost(n), bl(n, 0.0), best(n, 0.0);
-            for (int k = 0; k < n; k++) {
-                double c = 4.0 + (double)(S.cp[k + 1] - S.cp[k]) / 32.0;
-                for (int p = ptr[k]; p < ptr[k + 1]; p++) {
-                    const int j = dep[p];
-                    c += 2.0 + (double)(S.cp[j + 1] - S.dg[j] - 1) / 32.0;
-                }
-                cost[k] = c;
-            }
-            for (int k = n - 1; k >= 0; k--) {
-                bl[k] = cost[k] + best[k];
-                for (int p = ptr[k]; p < ptr[k + 1]; p++) best[dep[p]] = std::max(best[dep[p]], bl[k]);
-            }
-            std::vector<int> indeg(n), sptr(n + 1, 0), succ(dep.size());
-            for (int k = 0; k < n; k++) {
-                indeg[k] = ptr[k + 1] - ptr[k];
-                for (int p = ptr[k]; p < ptr[k + 1]; p++) sptr[dep[p] + 1]++;
-            }
-            for (int k = 0; k < n; k++) sptr[k + 1] += sptr[k];
-            {
-                std::vector<int> cur(sptr.begin(), sptr.end() - 1);
-                for (int k = 0; k < n; k++)
-                    for (int p = ptr[k]; p < ptr[k + 1]; p++) succ[cur[dep[p]]++] = k;
-            }
-            auto lower = [&bl](int a, int b) { return bl[a] < bl[b] || (bl[a] == bl[b] && a > b); };
-            std::vector<int> heap;
-            for (int k = 0; k < n; k++)
-                if (indeg[k] == 0) heap.push_back(k);
-            std::make_heap(heap.begin(), heap.end(), lower);
-            S.col_order.clear();
-            while (!heap.empty()) {
-                std::pop_heap(heap.begin(), heap.end(), lower);
-                const int k = heap.back();
-                heap.pop_back();
-                S.col_order.push_back(k);
-                for (int p = sptr[k]; p < sptr[k + 1]; p++)
-                    if (--indeg[succ[p]] == 0) {
-                        heap.push_back(succ[p]);
-                        std::push_heap(heap.begin(), heap.end(), lower);
-                    }
-            }
-        }
         long fl = 0, ga = 0;
         for (int k = 0; k < n; k++)
             for (int p = S.cp[k]; p < S.dg[k]; p++) {
