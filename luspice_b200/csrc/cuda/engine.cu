@@ -445,6 +445,13 @@ int sm_count() {
 
 static size_t smem_fixed(int nwords) { return 64 + (((size_t)nwords * 4 + 15) & ~(size_t)15) + 40 * sizeof(double); }
 
+// Dynamic shared memory of one solve CTA when ctas_per_sm share an SM.
+static size_t solve_smem_budget(int ctas_per_sm) {
+    size_t budget = 228 * 1024 / std::max(1, ctas_per_sm);
+    budget = budget > 1024 ? budget - 1024 : budget;
+    return std::min<size_t>(budget, 227 * 1024);
+}
+
 void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm, int m, int vsize,
                SmemPlan& plan) {
     int nmax = 1, levmax = 1, entmax = 4, rowmax = 4;
@@ -455,10 +462,7 @@ void make_plan(const std::vector<PatternObj*>& pats, int block, int ctas_per_sm,
         rowmax = std::max(rowmax, p->S.lev_max_rows);
     }
     (void)block;
-    const size_t limit = 227 * 1024;
-    size_t budget = 228 * 1024 / std::max(1, ctas_per_sm);
-    budget = budget > 1024 ? budget - 1024 : budget;
-    budget = std::min(budget, limit);
+    const size_t budget = solve_smem_budget(ctas_per_sm);
     plan.nwords = (nmax + 31) / 32;
     plan.m = m;
     plan.wcap = 0;
@@ -1035,6 +1039,10 @@ void ladder_bind(LaunchArgs& a, const LadderPlan& lp, char* mem, int* queue) {
     a.esc.ctl = queue + kLadderCtl;
 }
 
+// Triangular sweeps chosen by solve_sweep = 0: the dataflow sweeps whenever
+// the solve vectors fit shared memory.
+constexpr bool kAutoFlow = false;
+
 // Ladder slots when the options leave them at 0: every system of a batch up
 // to 256, else an eighth of them (at least 256).
 static int ladder_cap(const lusp_batch_opts& o, int nsys) {
@@ -1044,9 +1052,24 @@ static int ladder_cap(const lusp_batch_opts& o, int nsys) {
 
 int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, SmemPlan& plan) {
     make_plan(pats, o.block_threads, o.ctas_per_sm, o.krylov, o.prec == LUSP_FP64 ? 8 : 4, plan);
-    if (o.solve_sweep == 1) {   // dataflow sweeps only
-        plan.dcap = 0;
-        plan.sc_ent = plan.sc_rows = 0;
+    plan.flow = 0;
+    if (o.solve_sweep == 1 || (o.solve_sweep == 0 && kAutoFlow)) {
+        // Dataflow sweeps when every solve vector lives in shared memory and
+        // a second one fits where the stage ring would be (the ring then
+        // serves no system).
+        if (plan.ycap > 0) {
+            const size_t ring = plan.sc_ent ? kStages * stage_bytes(plan.sc_ent, plan.sc_rows, o.prec == LUSP_FP64 ? 8 : 4) : 0;
+            const size_t base = plan.bytes - ring;
+            if (base + 8 * (size_t)plan.ycap <= solve_smem_budget(o.ctas_per_sm)) {
+                plan.flow = 1;
+                plan.sc_ent = plan.sc_rows = 0;
+                plan.bytes = base + 8 * (size_t)plan.ycap;
+            }
+        }
+        if (!plan.flow && o.solve_sweep == 1) {   // per-row dataflow over global memory
+            plan.dcap = 0;
+            plan.sc_ent = plan.sc_rows = 0;
+        }
     }
     if (o.solve_sweep == 2 && plan.sc_ent == 0) {
         set_error("level-synchronous sweeps need a stage ring in shared memory");

@@ -226,6 +226,9 @@ struct SmemPlan {
     int ycap;                // doubles for a shared-memory solve vector
     int dcap;                // ints for shared-memory sweep descriptors
     int m;                   // Krylov dimension for H
+    int flow = 0;            // dataflow sweeps for shared-memory solve vectors
+                             // (second vector of ycap doubles in place of the
+                             // stage ring)
     size_t bytes;
 };
 

@@ -875,6 +875,27 @@ __device__ __forceinline__ double tail_row_dot(const VT* row, size_t stride, con
     return acc;
 }
 
+// The 32 factor values of one tail row's 32-column block (clamped
+// addresses, all loads in flight), and their dot product with y.
+template <typename VT>
+__device__ __forceinline__ void tail_load_regs(const VT* row, size_t stride, int w, VT* v) {
+#pragma unroll
+    for (int c = 0; c < 32; c++) v[c] = row[(size_t)min(c, w - 1) * stride];
+}
+// tail_row_dot as a call (rows past the ones a thread preloads: D above the
+// CTA size; keeps its 32 loads out of the caller's registers).
+template <typename VT>
+__device__ __noinline__ double tail_row_dot_call(const VT* row, size_t stride, const double* y, int w) {
+    return tail_row_dot<VT>(row, stride, y, w);
+}
+template <typename VT>
+__device__ __forceinline__ double tail_dot_regs(const VT* v, const double* y, int w) {
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 32; c++) acc = fma(c < w ? (double)v[c] : 0.0, y[min(c, w - 1)], acc);
+    return acc;
+}
+
 // y[k0..n) := L_tt^-1 y[k0..n) (unit lower; the tail rows' entries in the
 // columns before k0 were applied by the forward sweep's last level).
 template <typename VT>
@@ -883,30 +904,32 @@ __device__ __noinline__ void tail_forward(const PatternDev& P, const VT* T, doub
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     long long c_diag = 0, c_gemv = 0;
     double* yt = y + k0;
+    // Every thread loads one row of the block's 32 columns before the
+    // diagonal solve: warp 0 its row of the diagonal block, the other warps
+    // their first row below it (so those loads overlap the dependent chain
+    // of the diagonal solve).
+    const int nt = (int)blockDim.x - 32, t = (int)threadIdx.x - 32;
     for (int jb = 0; jb < D; jb += 32) {
         const int w = min(32, D - jb);
         const long long ta = clock64();
+        const int i0 = jb + w + t;
+        const bool pre = t >= 0 && i0 < D;
+        VT v[32];
+        if (warp == 0 || pre) tail_load_regs<VT>(T + (size_t)jb * ld + (warp == 0 ? jb + min(lane, w - 1) : i0), ld, w, v);
         if (warp == 0) {
-            double lr[32];
-            const int lr_ = min(lane, w - 1);
-            const VT* row = T + (size_t)jb * ld + jb + lr_;
-#pragma unroll
-            for (int c = 0; c < 32; c++) {
-                const double v = ValTraits<VT>::load(row + (size_t)min(c, w - 1) * ld);
-                lr[c] = (c < lane && lane < w) ? v : 0.0;
-            }
             double yr = lane < w ? yt[jb + lane] : 0.0;
 #pragma unroll
             for (int c = 0; c < 31; c++) {
                 const double yc = __shfl_sync(0xffffffffu, yr, c);
-                if (c < lane) yr = fma(-lr[c], yc, yr);
+                if (c < lane && lane < w) yr = fma(-(double)v[c], yc, yr);
             }
             if (lane < w) yt[jb + lane] = yr;
         }
         __syncthreads();
         const long long tb = clock64();
-        for (int i = jb + w + threadIdx.x; i < D; i += blockDim.x)
-            yt[i] -= tail_row_dot<VT>(T + (size_t)jb * ld + i, ld, yt + jb, w);
+        if (pre) yt[i0] -= tail_dot_regs<VT>(v, yt + jb, w);
+        for (int i = i0 + nt; t >= 0 && i < D; i += nt)
+            yt[i] -= tail_row_dot_call<VT>(T + (size_t)jb * ld + i, ld, yt + jb, w);
         __syncthreads();
         const long long tc = clock64();
         c_diag += tb - ta;
@@ -925,35 +948,37 @@ __device__ __noinline__ void tail_backward(const PatternDev& P, const VT* T, dou
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     long long c_diag = 0, c_gemv = 0;
     double* yt = y + k0;
+    // As tail_forward: warp 0 solves the diagonal block (each lane's
+    // reciprocal of its diagonal taken before the dependent chain), the
+    // other warps update the rows above it, their first row loaded before
+    // the diagonal solve.
+    const int nt = (int)blockDim.x - 32, t = (int)threadIdx.x - 32;
     for (int jb = ((D - 1) / 32) * 32; jb >= 0; jb -= 32) {
         const int w = min(32, D - jb);
         const long long ta = clock64();
+        const bool pre = t >= 0 && t < jb;
+        VT v[32];
+        const int lr_ = min(lane, w - 1);
+        if (warp == 0 || pre) tail_load_regs<VT>(T + (size_t)jb * ld + (warp == 0 ? jb + lr_ : t), ld, w, v);
         if (warp == 0) {
-            double ur[32];
-            const int lr_ = min(lane, w - 1);
-            const VT* row = T + (size_t)jb * ld + jb + lr_;
-#pragma unroll
-            for (int c = 0; c < 32; c++) {
-                const double v = ValTraits<VT>::load(row + (size_t)min(c, w - 1) * ld);
-                ur[c] = (c > lane && c < w) ? v : 0.0;
-            }
-            const double dgv = ValTraits<VT>::load(row + (size_t)lr_ * ld);
-            const double dg = lane < w ? dgv : 1.0;
+            const double dgv = ValTraits<VT>::load(T + (size_t)(jb + lr_) * ld + jb + lr_);
+            const double rdg = lane < w ? 1.0 / dgv : 1.0;
             double yr = lane < w ? yt[jb + lane] : 0.0;
 #pragma unroll
             for (int c = 31; c >= 0; c--) {
                 if (c < w) {
-                    if (lane == c) yr = yr / dg;
+                    if (lane == c) yr = yr * rdg;
                     const double zc = __shfl_sync(0xffffffffu, yr, c);
-                    if (lane < c) yr = fma(-ur[c], zc, yr);
+                    if (lane < c) yr = fma(-(double)v[c], zc, yr);
                 }
             }
             if (lane < w) yt[jb + lane] = yr;
         }
         __syncthreads();
         const long long tb = clock64();
-        for (int i = threadIdx.x; i < jb; i += blockDim.x)
-            yt[i] -= tail_row_dot<VT>(T + (size_t)jb * ld + i, ld, yt + jb, w);
+        if (pre) yt[t] -= tail_dot_regs<VT>(v, yt + jb, w);
+        for (int i = t + nt; t >= 0 && i < jb; i += nt)
+            yt[i] -= tail_row_dot_call<VT>(T + (size_t)jb * ld + i, ld, yt + jb, w);
         __syncthreads();
         const long long tc = clock64();
         c_diag += tb - ta;
@@ -1244,7 +1269,8 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
 // nfl x int4][bwd level descriptors nbl x int4][fwd lanes nfl][bwd lanes
 // nbl][fwd_order n][fwd rp n+1][bwd_order n][bwd rp n+1].
 __device__ __forceinline__ bool sweep_desc_fits(const PatternDev& P, const SmemPlan& plan) {
-    return P.n <= plan.ycap && 4 * P.n + 5 * (P.nfwd_levels + P.nbwd_levels) + 4 <= plan.dcap && plan.sc_ent > 0;
+    return P.n <= plan.ycap && 4 * P.n + 5 * (P.nfwd_levels + P.nbwd_levels) + 4 <= plan.dcap &&
+           (plan.sc_ent > 0 || plan.flow);
 }
 
 // Byte offset (16-byte aligned) of the sweep descriptors in the solve
@@ -1355,14 +1381,161 @@ __device__ void cta_lu_apply_levels(const SysDev& S, const PatternDev& P, const 
     }
 }
 
-// Dispatch: level-synchronous sweeps when the launch has a stage ring
-// (sd != nullptr: descriptors in shared memory when they fit, else read
-// from the pattern in global memory), else the dataflow version.
+// ---------------------------------------------------------------------------
+// Dataflow triangular sweeps with the solve vector in shared memory.  Warp w
+// takes the rows w, w + NW, w + 2 NW, ... of a sweep order.  The order is
+// level-sorted, so every dependency of a row comes before it; the smallest
+// unfinished row therefore always has its dependencies done and its warp at
+// it (a warp's earlier rows are smaller), and the sweep cannot deadlock.
+// There is no CTA barrier inside a sweep and no ready flag: every output
+// slot starts as a signalling-NaN bit pattern, which arithmetic never
+// produces, a row's result is one 8-byte store, and a reader polls the value
+// it needs.  A warp loads the next row's header, right-hand side and first
+// 32 entries while it works on the current row; longer rows load four
+// chunks of 32 at a time.
+// ---------------------------------------------------------------------------
+constexpr long long kFlowSentinel = 0x7ff00000deadbeefll;   // signalling NaN
+
+// out[j] once written (bounded wait: after kSpinLimit polls, or at once when
+// *abort is set, the wait gives up, sets ST_WAIT_TIMEOUT and returns the
+// sentinel, a NaN).
+__device__ __noinline__ double flow_wait(const double* out, int j, int* abort, int& bad) {
+    const volatile long long* w = (const volatile long long*)out + j;
+    const volatile int* ab = abort;
+    long long v, it = 0;
+    while ((v = *w) == kFlowSentinel) {
+        if (++it > 32) {
+            if (*ab) break;
+            if (it > kSpinLimit) {
+                atomicExch(abort, 1);
+                break;
+            }
+            __nanosleep(32);
+        }
+    }
+    if (v == kFlowSentinel) bad |= ST_WAIT_TIMEOUT;
+    return __longlong_as_double(v);
+}
+
+__device__ __forceinline__ double flow_take(const double* out, int j, long long raw, int* abort, int& bad) {
+    return raw != kFlowSentinel ? __longlong_as_double(raw) : flow_wait(out, j, abort, bad);
+}
+
+// out[order[r]] := (rhs[order[r]] - sum_e val[e] out[ci[e]]) (* rdg[r] for
+// U) over the rows r < nrows of a sweep order, entries e in [rp[r], rp[r+1]).
+template <typename VT, bool UPPER>
+__device__ __noinline__ void flow_sweep(int nrows, const int* order, const int* rp, const int* ci, const VT* val,
+                                        const VT* rdg, const double* rhs, double* out, int* abort, int& bad) {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const volatile long long* vo = (const volatile long long*)out;
+    int idx = threadIdx.x >> 5;
+    int i = 0, p0 = 0, e = 0, j = -1;
+    double v = 0.0, b = 0.0, d = 1.0;
+    if (idx < nrows) {
+        i = order[idx];
+        p0 = rp[idx];
+        e = rp[idx + 1];
+        j = p0 + lane < e ? ci[p0 + lane] : -1;
+        v = j >= 0 ? ValTraits<VT>::load(val + p0 + lane) : 0.0;
+        b = rhs[i];
+        if (UPPER) d = ValTraits<VT>::load(rdg + idx);
+    }
+    while (idx < nrows) {
+        // The next row of this warp, in flight while this one is computed.
+        const int nx = idx + nw;
+        int i2 = 0, q0 = 0, e2 = 0, j2 = -1;
+        double v2 = 0.0, b2 = 0.0, d2 = 1.0;
+        if (nx < nrows) {
+            i2 = order[nx];
+            q0 = rp[nx];
+            e2 = rp[nx + 1];
+            j2 = q0 + lane < e2 ? ci[q0 + lane] : -1;
+            v2 = j2 >= 0 ? ValTraits<VT>::load(val + q0 + lane) : 0.0;
+            b2 = rhs[i2];
+            if (UPPER) d2 = ValTraits<VT>::load(rdg + nx);
+        }
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        if (j >= 0) a0 = fma(v, flow_take(out, j, vo[j], abort, bad), a0);
+        for (int base = p0 + 32; base < e; base += 128) {
+            int jj[4];
+            double vv[4];
+            long long raw[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int p = base + 32 * q + lane;
+                jj[q] = p < e ? ci[p] : -1;
+                vv[q] = p < e ? ValTraits<VT>::load(val + p) : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) raw[q] = jj[q] >= 0 ? vo[jj[q]] : 0ll;
+            if (jj[0] >= 0) a0 = fma(vv[0], flow_take(out, jj[0], raw[0], abort, bad), a0);
+            if (jj[1] >= 0) a1 = fma(vv[1], flow_take(out, jj[1], raw[1], abort, bad), a1);
+            if (jj[2] >= 0) a2 = fma(vv[2], flow_take(out, jj[2], raw[2], abort, bad), a2);
+            if (jj[3] >= 0) a3 = fma(vv[3], flow_take(out, jj[3], raw[3], abort, bad), a3);
+        }
+        const double acc = warp_sum((a0 + a1) + (a2 + a3));
+        if (lane == 0) {
+            const double r = b - acc;
+            ((volatile double*)out)[i] = UPPER ? r * d : r;
+        }
+        idx = nx;
+        i = i2;
+        p0 = q0;
+        e = e2;
+        j = j2;
+        v = v2;
+        b = b2;
+        d = d2;
+    }
+}
+
+// y := U^-1 L^-1 rhs with the dataflow sweeps: forward into y, the dense
+// trailing block in place, backward into y2 (n doubles of shared memory),
+// copied back to y.
+template <typename VT>
+__device__ void cta_lu_apply_flow(const SysDev& S, const PatternDev& P, const SweepDesc& sd, const double* rhs,
+                                  double* y, double* y2, Smem& sm, int& bad) {
+    const int n = P.n, k0 = P.k0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) ((long long*)y)[i] = kFlowSentinel;
+    if (threadIdx.x == 0) sm.ctl[3] = 0;
+    __syncthreads();
+    const long long t0 = clock64();
+    flow_sweep<VT, false>(n, sd.f_ord, sd.f_rp, P.lci, (const VT*)S.lval, (const VT*)nullptr, rhs, y, &sm.ctl[3],
+                          bad);
+    __syncthreads();
+    const long long t1 = clock64();
+    if (P.dtail > 0) {
+        tail_forward<VT>(P, (const VT*)S.tail, y, S.stats);
+        tail_backward<VT>(P, (const VT*)S.tail, y, S.stats);
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        ((long long*)y2)[i] = i < k0 ? kFlowSentinel : __double_as_longlong(y[i]);
+    __syncthreads();
+    const long long t2 = clock64();
+    flow_sweep<VT, true>(k0, sd.b_ord, sd.b_rp, P.uci, (const VT*)S.uval, (const VT*)S.udiag_bwd, y, y2,
+                         &sm.ctl[3], bad);
+    __syncthreads();
+    for (int i = threadIdx.x; i < k0; i += blockDim.x) y[i] = y2[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        S.stats->cyc_lsolve += t1 - t0;
+        S.stats->cyc_tail += t2 - t1;
+        S.stats->cyc_usolve += clock64() - t2;
+    }
+}
+
+// Dispatch: the dataflow sweeps of shared-memory solve vectors when the
+// plan chose them (the second vector where the stage ring would be), else
+// level-synchronous sweeps when the launch has a stage ring (sd != nullptr:
+// descriptors in shared memory when they fit, else read from the pattern in
+// global memory), else the per-row dataflow version over global memory.
 template <typename VT>
 __device__ __forceinline__ void lu_apply(const SysDev& S, const SmemPlan& plan, const double* rhs,
                                          double* y, Smem& sm, const SweepDesc* sd, int& bad) {
     const PatternDev& P = *S.pat;
-    if (sd) cta_lu_apply_levels<VT>(S, P, plan, rhs, y, *sd, sweep_stage_base(plan, sm), sm.red);
+    if (plan.flow && sd && P.n <= plan.ycap)
+        cta_lu_apply_flow<VT>(S, P, *sd, rhs, y, (double*)sweep_stage_base(plan, sm), sm, bad);
+    else if (sd) cta_lu_apply_levels<VT>(S, P, plan, rhs, y, *sd, sweep_stage_base(plan, sm), sm.red);
     else cta_lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, (const VT*)S.tail, rhs,
                           y, sm, bad, S.stats);
 }
@@ -1378,7 +1551,7 @@ __device__ const SweepDesc* prepare_sweeps(const PatternDev& P, const SmemPlan& 
         load_sweep_desc(P, d);
         *buf = SweepDesc(P, d);
         sd = buf;
-    } else if (plan.sc_ent > 0) {
+    } else if (plan.sc_ent > 0 || plan.flow) {
         *buf = SweepDesc(P);
         sd = buf;
     }
