@@ -882,6 +882,10 @@ void fill_params(SolveParams& prm, const lusp_batch_opts& o) {
 // 227 M; the n = 4050 power grid, refactored faster by one 2-SM cluster,
 // has 5.9 M).
 constexpr long long kSpreadMinUpdates = 16ll << 20;
+// Gathered updates per system above which a batch of at most one system
+// per SM spreads each system over up to kSpreadMidGroup 256-thread CTAs.
+constexpr long long kSpreadMidUpdates = 1ll << 17;
+constexpr int kSpreadMidGroup = 12;
 
 int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, int nsys, LaunchArgs& a) {
     a.rblock = refactor_block(o, nsys);
@@ -920,9 +924,30 @@ int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& 
         }
         const int slots = occ * sm_count();
         int g = 0;
+        bool mid = false;
         if (o.refactor_spread > 0) g = std::min(o.refactor_spread, slots / std::max(1, nsys));
         else if (nsys * 8 <= sm_count() && gmin >= kSpreadMinUpdates) g = slots / nsys;
-        if (g >= 2 && o.refactor_threads <= 0) {
+        else if (nsys <= sm_count() && gmin >= kSpreadMidUpdates && o.refactor_threads <= 0 &&
+                 o.refactor_cluster <= 0) {
+            // Medium systems, at most one per SM: 256-thread CTAs, four per
+            // SM, up to kSpreadMidGroup per system (B200, 50 systems: the
+            // n = 4050 grid 2.22 -> 1.95 ms, an n = 4000 circuit 0.82 ->
+            // 0.70 ms against one 2-CTA cluster each; the n = 989 circuit,
+            // 41 k updates, gains nothing).
+            SmemPlan pl;
+            make_refactor_plan(pats, 256, o.prec == LUSP_FP64 ? 8 : 4, pl);
+            int mocc = 0;
+            rc = refactor_occupancy(o.prec, pl.bytes, 256, &mocc, true);
+            if (rc != LUSP_OK) return rc;
+            const int mg = std::min(kSpreadMidGroup, mocc * sm_count() / nsys);
+            if (mg >= 4) {
+                g = mg;
+                mid = true;
+                a.rblock = 256;
+                a.rplan = pl;
+            }
+        }
+        if (g >= 2 && o.refactor_threads <= 0 && !mid) {
             // One CTA per SM, of the size whose per-warp work area holds the
             // longest column before the dense block (longer ones spill to
             // global memory).
@@ -1055,15 +1080,17 @@ int plan_for(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o, Sme
     plan.flow = 0;
     if (o.solve_sweep == 1 || (o.solve_sweep == 0 && kAutoFlow)) {
         // Dataflow sweeps when every solve vector lives in shared memory and
-        // a second one fits where the stage ring would be (the ring then
-        // serves no system).
+        // a second one and the warps' staging rings fit where the level
+        // sweeps' stage ring would be (that ring then serves no system).
         if (plan.ycap > 0) {
             const size_t ring = plan.sc_ent ? kStages * stage_bytes(plan.sc_ent, plan.sc_rows, o.prec == LUSP_FP64 ? 8 : 4) : 0;
             const size_t base = plan.bytes - ring;
-            if (base + 8 * (size_t)plan.ycap <= solve_smem_budget(o.ctas_per_sm)) {
+            const size_t need = (((size_t)plan.ycap * 8 + 15) & ~(size_t)15) +
+                                flow_ring_bytes(o.block_threads / 32, o.prec == LUSP_FP64 ? 8 : 4);
+            if (base + need <= solve_smem_budget(o.ctas_per_sm)) {
                 plan.flow = 1;
                 plan.sc_ent = plan.sc_rows = 0;
-                plan.bytes = base + 8 * (size_t)plan.ycap;
+                plan.bytes = base + need;
             }
         }
         if (!plan.flow && o.solve_sweep == 1) {   // per-row dataflow over global memory

@@ -1390,11 +1390,21 @@ __device__ void cta_lu_apply_levels(const SysDev& S, const PatternDev& P, const 
 // There is no CTA barrier inside a sweep and no ready flag: every output
 // slot starts as a signalling-NaN bit pattern, which arithmetic never
 // produces, a row's result is one 8-byte store, and a reader polls the value
-// it needs.  A warp loads the next row's header, right-hand side and first
-// 32 entries while it works on the current row; longer rows load four
-// chunks of 32 at a time.
+// it needs.  Each warp stages its own rows in a private ring of
+// kFlowSlots shared-memory slots, kFlowSlots - 1 rows ahead, by cp.async
+// (column indices, values, the right-hand side and the reciprocal
+// diagonal; a row's entries past kFlowCap are read from global memory, four
+// chunks of 32 in flight), so a row waits only for its dependencies.
 // ---------------------------------------------------------------------------
 constexpr long long kFlowSentinel = 0x7ff00000deadbeefll;   // signalling NaN
+constexpr int kFlowSlots = 3, kFlowCap = 128;
+
+// One ring slot: kFlowCap column indices, kFlowCap values, the row's
+// right-hand side (fp64) and its reciprocal diagonal (VT).
+__host__ __device__ inline size_t flow_slot_bytes(int vsize) { return (size_t)kFlowCap * (4 + vsize) + 16; }
+__host__ __device__ inline size_t flow_ring_bytes(int nwarps, int vsize) {
+    return (size_t)nwarps * kFlowSlots * flow_slot_bytes(vsize);
+}
 
 // out[j] once written (bounded wait: after kSpinLimit polls, or at once when
 // *abort is set, the wait gives up, sets ST_WAIT_TIMEOUT and returns the
@@ -1421,87 +1431,105 @@ __device__ __forceinline__ double flow_take(const double* out, int j, long long 
     return raw != kFlowSentinel ? __longlong_as_double(raw) : flow_wait(out, j, abort, bad);
 }
 
+// Four entries per lane: sum into a[0..3] of v * out[j] (j < 0: none).
+__device__ __forceinline__ void flow_acc4(const int* jj, const double* vv, const double* out, int* abort, int& bad,
+                                          double* a) {
+    const volatile long long* vo = (const volatile long long*)out;
+    long long raw[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) raw[q] = jj[q] >= 0 ? vo[jj[q]] : 0ll;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        if (jj[q] >= 0) a[q] = fma(vv[q], flow_take(out, jj[q], raw[q], abort, bad), a[q]);
+}
+
 // out[order[r]] := (rhs[order[r]] - sum_e val[e] out[ci[e]]) (* rdg[r] for
 // U) over the rows r < nrows of a sweep order, entries e in [rp[r], rp[r+1]).
+// ring: this CTA's staging area (flow_ring_bytes).  rhs may be global or
+// shared memory.
 template <typename VT, bool UPPER>
 __device__ __noinline__ void flow_sweep(int nrows, const int* order, const int* rp, const int* ci, const VT* val,
-                                        const VT* rdg, const double* rhs, double* out, int* abort, int& bad) {
-    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const volatile long long* vo = (const volatile long long*)out;
-    int idx = threadIdx.x >> 5;
-    int i = 0, p0 = 0, e = 0, j = -1;
-    double v = 0.0, b = 0.0, d = 1.0;
-    if (idx < nrows) {
-        i = order[idx];
-        p0 = rp[idx];
-        e = rp[idx + 1];
-        j = p0 + lane < e ? ci[p0 + lane] : -1;
-        v = j >= 0 ? ValTraits<VT>::load(val + p0 + lane) : 0.0;
-        b = rhs[i];
-        if (UPPER) d = ValTraits<VT>::load(rdg + idx);
-    }
-    while (idx < nrows) {
-        // The next row of this warp, in flight while this one is computed.
-        const int nx = idx + nw;
-        int i2 = 0, q0 = 0, e2 = 0, j2 = -1;
-        double v2 = 0.0, b2 = 0.0, d2 = 1.0;
-        if (nx < nrows) {
-            i2 = order[nx];
-            q0 = rp[nx];
-            e2 = rp[nx + 1];
-            j2 = q0 + lane < e2 ? ci[q0 + lane] : -1;
-            v2 = j2 >= 0 ? ValTraits<VT>::load(val + q0 + lane) : 0.0;
-            b2 = rhs[i2];
-            if (UPPER) d2 = ValTraits<VT>::load(rdg + nx);
+                                        const VT* rdg, const double* rhs, double* out, char* ring, int* abort,
+                                        int& bad) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const size_t sb = flow_slot_bytes(sizeof(VT));
+    char* my = ring + (size_t)warp * kFlowSlots * sb;
+    const bool rglob = __isGlobal(rhs);
+    auto issue = [&](int k) {
+        const int idx = warp + k * nw;
+        if (idx < nrows) {
+            const int b = rp[idx], m = min(rp[idx + 1] - b, kFlowCap);
+            char* s = my + (size_t)(k % kFlowSlots) * sb;
+            int* sc = (int*)s;
+            VT* sv = (VT*)(s + (size_t)kFlowCap * 4);
+            double* sx = (double*)(s + (size_t)kFlowCap * (4 + sizeof(VT)));
+            for (int t = lane; t < m; t += 32) {
+                cp_async_4(sc + t, ci + b + t);
+                cp_async_val(sv + t, val + b + t);
+            }
+            if (lane == 0 && rglob) cp_async_8(sx, rhs + order[idx]);
+            if (UPPER && lane == 1) cp_async_val((VT*)(sx + 1), rdg + idx);
         }
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-        if (j >= 0) a0 = fma(v, flow_take(out, j, vo[j], abort, bad), a0);
-        for (int base = p0 + 32; base < e; base += 128) {
+        cp_async_commit();
+    };
+    for (int k = 0; k < kFlowSlots - 1; k++) issue(k);
+    for (int k = 0, idx = warp; idx < nrows; k++, idx += nw) {
+        issue(k + kFlowSlots - 1);
+        cp_async_wait_group<kFlowSlots - 1>();
+        __syncwarp();
+        const char* s = my + (size_t)(k % kFlowSlots) * sb;
+        const int* sc = (const int*)s;
+        const VT* sv = (const VT*)(s + (size_t)kFlowCap * 4);
+        const double* sx = (const double*)(s + (size_t)kFlowCap * (4 + sizeof(VT)));
+        const int i = order[idx], b = rp[idx], e = rp[idx + 1];
+        const int m = min(e - b, kFlowCap);
+        double a[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int t0 = lane; t0 < m; t0 += 128) {
             int jj[4];
             double vv[4];
-            long long raw[4];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const int p = base + 32 * q + lane;
+                const int t = t0 + 32 * q;
+                jj[q] = t < m ? sc[t] : -1;
+                vv[q] = t < m ? ValTraits<VT>::load(sv + t) : 0.0;
+            }
+            flow_acc4(jj, vv, out, abort, bad, a);
+        }
+        for (int p0 = b + kFlowCap + lane; p0 < e; p0 += 128) {
+            int jj[4];
+            double vv[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int p = p0 + 32 * q;
                 jj[q] = p < e ? ci[p] : -1;
                 vv[q] = p < e ? ValTraits<VT>::load(val + p) : 0.0;
             }
-#pragma unroll
-            for (int q = 0; q < 4; q++) raw[q] = jj[q] >= 0 ? vo[jj[q]] : 0ll;
-            if (jj[0] >= 0) a0 = fma(vv[0], flow_take(out, jj[0], raw[0], abort, bad), a0);
-            if (jj[1] >= 0) a1 = fma(vv[1], flow_take(out, jj[1], raw[1], abort, bad), a1);
-            if (jj[2] >= 0) a2 = fma(vv[2], flow_take(out, jj[2], raw[2], abort, bad), a2);
-            if (jj[3] >= 0) a3 = fma(vv[3], flow_take(out, jj[3], raw[3], abort, bad), a3);
+            flow_acc4(jj, vv, out, abort, bad, a);
         }
-        const double acc = warp_sum((a0 + a1) + (a2 + a3));
+        const double acc = warp_sum((a[0] + a[1]) + (a[2] + a[3]));
         if (lane == 0) {
-            const double r = b - acc;
-            ((volatile double*)out)[i] = UPPER ? r * d : r;
+            const double r = (rglob ? sx[0] : rhs[i]) - acc;
+            ((volatile double*)out)[i] = UPPER ? r * ValTraits<VT>::load((const VT*)(sx + 1)) : r;
         }
-        idx = nx;
-        i = i2;
-        p0 = q0;
-        e = e2;
-        j = j2;
-        v = v2;
-        b = b2;
-        d = d2;
+        __syncwarp();   // the slot is staged again by the next issue
     }
+    cp_async_wait_all();
+    __syncwarp();
 }
 
 // y := U^-1 L^-1 rhs with the dataflow sweeps: forward into y, the dense
 // trailing block in place, backward into y2 (n doubles of shared memory),
-// copied back to y.
+// copied back to y.  ring: the staging area of flow_sweep.
 template <typename VT>
 __device__ void cta_lu_apply_flow(const SysDev& S, const PatternDev& P, const SweepDesc& sd, const double* rhs,
-                                  double* y, double* y2, Smem& sm, int& bad) {
+                                  double* y, double* y2, char* ring, Smem& sm, int& bad) {
     const int n = P.n, k0 = P.k0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) ((long long*)y)[i] = kFlowSentinel;
     if (threadIdx.x == 0) sm.ctl[3] = 0;
     __syncthreads();
     const long long t0 = clock64();
-    flow_sweep<VT, false>(n, sd.f_ord, sd.f_rp, P.lci, (const VT*)S.lval, (const VT*)nullptr, rhs, y, &sm.ctl[3],
-                          bad);
+    flow_sweep<VT, false>(n, sd.f_ord, sd.f_rp, P.lci, (const VT*)S.lval, (const VT*)nullptr, rhs, y, ring,
+                          &sm.ctl[3], bad);
     __syncthreads();
     const long long t1 = clock64();
     if (P.dtail > 0) {
@@ -1512,7 +1540,7 @@ __device__ void cta_lu_apply_flow(const SysDev& S, const PatternDev& P, const Sw
         ((long long*)y2)[i] = i < k0 ? kFlowSentinel : __double_as_longlong(y[i]);
     __syncthreads();
     const long long t2 = clock64();
-    flow_sweep<VT, true>(k0, sd.b_ord, sd.b_rp, P.uci, (const VT*)S.uval, (const VT*)S.udiag_bwd, y, y2,
+    flow_sweep<VT, true>(k0, sd.b_ord, sd.b_rp, P.uci, (const VT*)S.uval, (const VT*)S.udiag_bwd, y, y2, ring,
                          &sm.ctl[3], bad);
     __syncthreads();
     for (int i = threadIdx.x; i < k0; i += blockDim.x) y[i] = y2[i];
@@ -1522,6 +1550,15 @@ __device__ void cta_lu_apply_flow(const SysDev& S, const PatternDev& P, const Sw
         S.stats->cyc_tail += t2 - t1;
         S.stats->cyc_usolve += clock64() - t2;
     }
+}
+
+// Second solve vector and staging ring of the dataflow sweeps, where the
+// level sweeps' stage ring would be.
+__device__ __forceinline__ double* flow_y2_base(const SmemPlan& plan, Smem& sm) {
+    return (double*)sweep_stage_base(plan, sm);
+}
+__device__ __forceinline__ char* flow_ring_base(const SmemPlan& plan, Smem& sm) {
+    return (char*)sweep_stage_base(plan, sm) + (((size_t)plan.ycap * 8 + 15) & ~(size_t)15);
 }
 
 // Dispatch: the dataflow sweeps of shared-memory solve vectors when the
@@ -1534,7 +1571,7 @@ __device__ __forceinline__ void lu_apply(const SysDev& S, const SmemPlan& plan, 
                                          double* y, Smem& sm, const SweepDesc* sd, int& bad) {
     const PatternDev& P = *S.pat;
     if (plan.flow && sd && P.n <= plan.ycap)
-        cta_lu_apply_flow<VT>(S, P, *sd, rhs, y, (double*)sweep_stage_base(plan, sm), sm, bad);
+        cta_lu_apply_flow<VT>(S, P, *sd, rhs, y, flow_y2_base(plan, sm), flow_ring_base(plan, sm), sm, bad);
     else if (sd) cta_lu_apply_levels<VT>(S, P, plan, rhs, y, *sd, sweep_stage_base(plan, sm), sm.red);
     else cta_lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, (const VT*)S.tail, rhs,
                           y, sm, bad, S.stats);
