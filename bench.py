@@ -736,8 +736,17 @@ def main():
         batch.time_kernels(False)
         return {k: statistics.mean(d[k] for d in kms) for k in ("refactor", "dense", "solve")}
 
+    def refactor_kernel_name(batch):
+        sh = batch.launch_shape()
+        if sh["refactor_spread"] > 0:
+            return (f"refactor_spread_kernel<float> ({sh['refactor_spread']} CTAs of {sh['refactor_block']} "
+                    f"threads per system, {sh['refactor_grid']} CTAs)")
+        return (f"refactor_kernel<float> ({sh['refactor_cluster']}-CTA cluster of {sh['refactor_block']} threads "
+                f"per system, {sh['refactor_grid']} CTAs)")
+
     kt = kernel_times(B)
     kt64 = kernel_times(B64)
+    ref_kernel = refactor_kernel_name(B)
     refactor_ms, dense_ms, solve_ms = kt["refactor"], kt["dense"], kt["solve"]
     achieved_ref = alg_ref / (refactor_ms / 1000.0) / 1e9
     achieved = alg / (solve_ms / 1000.0) / 1e9
@@ -874,8 +883,8 @@ def main():
                                         "results_equal_device_timed": e2e_same}},
             "roofline": {"bound": "hbm", "achieved": achieved_ref, "peak": hbm, "unit": "GB/s",
                          "frac": achieved_ref / hbm,
-                         "traffic": traffic_of("refactor_kernel_power_grid4050x50.json"),
-                         "peak_kind": peak_kind, "kernel": "refactor_kernel<float,768>",
+                         "traffic": traffic_of("refactor_spread_kernel_power_grid4050x50.json"),
+                         "peak_kind": peak_kind, "kernel": ref_kernel,
                          "alg_bytes_per_launch": alg_ref, "kernel_ms": refactor_ms,
                          "dense_kernel_ms": dense_ms,
                          "solve_kernel": {"achieved": achieved, "frac": achieved / hbm,

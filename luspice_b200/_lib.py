@@ -139,6 +139,7 @@ SIGNATURES = {
     "lusp_batch_launch_count": (C.c_int, [C.c_void_p]),
     "lusp_batch_time_kernels": (C.c_int, [C.c_void_p, C.c_int]),
     "lusp_batch_kernel_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "lusp_batch_launch_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "lusp_sell_create": (C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, C.c_int, C.c_int,
                                    C.c_int, c_void_pp]),
     "lusp_sell_destroy": (None, [C.c_void_p]),

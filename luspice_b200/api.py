@@ -205,6 +205,14 @@ class Batch:
         _check(L.load().lusp_batch_kernel_ms(self.handle, ms), "kernel_ms")
         return {"refactor": ms[0], "dense": ms[1], "solve": ms[2]}
 
+    def launch_shape(self) -> dict:
+        """The launch shape the library chose for this batch."""
+        v = (C.c_int * 9)()
+        _check(L.load().lusp_batch_launch_shape(self.handle, v), "launch_shape")
+        keys = ("refactor_grid", "refactor_block", "refactor_cluster", "refactor_spread", "dense_grid",
+                "dense_block", "solve_grid", "solve_block", "sweeps")
+        return dict(zip(keys, list(v)))
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             L.load().lusp_batch_destroy(self.handle)

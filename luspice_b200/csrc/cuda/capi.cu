@@ -337,6 +337,22 @@ int lusp_batch_launch_count(const lusp_batch* hb) {
     return B ? B->launches : 0;
 }
 
+int lusp_batch_launch_shape(const lusp_batch* hb, int* shape) {
+    const BatchObj* B = BO(hb);
+    if (!B || !shape) return LUSP_EARG;
+    const lusp::LaunchArgs& a = B->launch;
+    shape[0] = a.rgrid;
+    shape[1] = a.rblock;
+    shape[2] = a.rcluster;
+    shape[3] = a.rspread.group;
+    shape[4] = a.dgrid;
+    shape[5] = a.dblock;
+    shape[6] = a.grid;
+    shape[7] = a.block;
+    shape[8] = a.plan.flow || a.plan.sc_ent == 0 ? 1 : 2;
+    return LUSP_OK;
+}
+
 int lusp_batch_time_kernels(lusp_batch* hb, int on) {
     BatchObj* B = BO(hb);
     if (!B) return LUSP_EARG;

@@ -1142,6 +1142,11 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
     const int warp = threadIdx.x >> 5;
     const bool pow2 = (NT & (NT - 1)) == 0;
     const int lgb = 31 - __clz(NT);
+    // The copies are issued from the highest threads down: rows go to the
+    // lowest warps, so in a narrow level the warps that issue are not the
+    // ones that compute (issuing a level's copies takes a warp ~500 cycles,
+    // which sat on the critical warp 0 of every level).
+    const int itid = NT - 1 - (int)threadIdx.x;
     auto issue = [&](int L) {
         if (L < nlev) {
             const int4 d = ld4[L];
@@ -1151,14 +1156,14 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
                 VT* sv = (VT*)(base + (size_t)CE * 4);
                 VT* sd = (VT*)(base + (size_t)CE * (4 + sizeof(VT)));
                 const int a0 = d.z & ~3, n4 = ((d.w + 3) & ~3) - a0;
-                for (int t = threadIdx.x * 4; t < n4; t += NT * 4) {
+                for (int t = itid * 4; t < n4; t += NT * 4) {
                     cp_async_16(sc + t, ci + a0 + t);
                     cp_async_16(sv + t, val + a0 + t);
                     if (sizeof(VT) == 8) cp_async_16(sv + t + 2, val + a0 + t + 2);
                 }
                 if (UPPER) {
                     const int b0 = d.x & ~3, m4 = ((d.y + 3) & ~3) - b0;
-                    for (int t = threadIdx.x * 4; t < m4; t += NT * 4) {
+                    for (int t = itid * 4; t < m4; t += NT * 4) {
                         cp_async_16(sd + t, dgo + b0 + t);
                         if (sizeof(VT) == 8) cp_async_16(sd + t + 2, dgo + b0 + t + 2);
                     }
@@ -1243,22 +1248,36 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
             const int rbase = r0 + rd * ngr;
             if (rbase + ((warp * 32) >> lg) >= r1) break;   // nothing left for this warp
             const int r = rbase + ((int)threadIdx.x >> lg);
-            double acc = 0.0;
+            double acc = 0.0, yi = 0.0, di = 1.0;
+            int i = 0;
             if (r < r1) {
+                // The row's own right-hand side and diagonal, loaded beside
+                // the dot product instead of after its reduction (no other
+                // thread writes y[i] in this level).
+                if (lig == 0) {
+                    i = order[r];
+                    yi = y[i];
+                    if (UPPER) di = ValTraits<VT>::load(dd + (r - rb));
+                }
                 if (GY) {
                     acc = row_dot<VT>(vv, cc, y, rp[r] - eb + lig, rp[r + 1] - eb, g);
                 } else {
+                    // Two entries per lane in flight.
                     const int pe = rp[r + 1] - eb;
-                    for (int e = rp[r] - eb + lig; e < pe; e += g)
-                        acc = fma(ValTraits<VT>::load(vv + e), y[cc[e]], acc);
+                    int e = rp[r] - eb + lig;
+                    double a1 = 0.0;
+                    for (; e + g < pe; e += 2 * g) {
+                        const int c0 = cc[e], c1 = cc[e + g];
+                        const double v0 = ValTraits<VT>::load(vv + e), v1 = ValTraits<VT>::load(vv + e + g);
+                        acc = fma(v0, y[c0], acc);
+                        a1 = fma(v1, y[c1], a1);
+                    }
+                    if (e < pe) acc = fma(ValTraits<VT>::load(vv + e), y[cc[e]], acc);
+                    acc += a1;
                 }
             }
             for (int o = g >> 1; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, g);
-            if (r < r1 && lig == 0) {
-                const int i = order[r];
-                if (UPPER) y[i] = (y[i] - acc) * ValTraits<VT>::load(dd + (r - rb));
-                else y[i] = y[i] - acc;
-            }
+            if (r < r1 && lig == 0) y[i] = UPPER ? (yi - acc) * di : yi - acc;
         }
     }
     cp_async_wait_all();
