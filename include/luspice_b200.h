@@ -248,12 +248,13 @@ int lusp_batch_launch_count(const lusp_batch *b);
  * launch; LUSP_EARG while timing is off). */
 int lusp_batch_time_kernels(lusp_batch *b, int on);
 int lusp_batch_kernel_ms(lusp_batch *b, float *ms3);
-/* Launch shape the batch chose (for reports): shape[0..8] = refactor grid,
+/* Launch shape the batch chose (for reports): shape[0..9] = refactor grid,
  * refactor CTA threads, CTAs per system in one thread-block cluster, CTAs
  * per system in spread mode (0: none; the refactor_spread_kernel instance
  * runs), dense-block grid (0: no dense block) and CTA threads, solve grid
- * and CTA threads, triangular sweeps (1 dataflow, 2 level-synchronous). */
-int lusp_batch_launch_shape(const lusp_batch *b, int *shape9);
+ * and CTA threads, triangular sweeps (1 dataflow, 2 level-synchronous),
+ * dense-block CTAs per system (a thread-block cluster when 2). */
+int lusp_batch_launch_shape(const lusp_batch *b, int *shape10);
 
 /* ---- serving loop ----
  * Continuous batching of refactor+solve requests from concurrent callers

@@ -207,10 +207,10 @@ class Batch:
 
     def launch_shape(self) -> dict:
         """The launch shape the library chose for this batch."""
-        v = (C.c_int * 9)()
+        v = (C.c_int * 10)()
         _check(L.load().lusp_batch_launch_shape(self.handle, v), "launch_shape")
         keys = ("refactor_grid", "refactor_block", "refactor_cluster", "refactor_spread", "dense_grid",
-                "dense_block", "solve_grid", "solve_block", "sweeps")
+                "dense_block", "solve_grid", "solve_block", "sweeps", "dense_cluster")
         return dict(zip(keys, list(v)))
 
     def close(self) -> None:

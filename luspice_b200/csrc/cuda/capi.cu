@@ -350,6 +350,7 @@ int lusp_batch_launch_shape(const lusp_batch* hb, int* shape) {
     shape[6] = a.grid;
     shape[7] = a.block;
     shape[8] = a.plan.flow || a.plan.sc_ent == 0 ? 1 : 2;
+    shape[9] = a.dcluster;
     return LUSP_OK;
 }
 

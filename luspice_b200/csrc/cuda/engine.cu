@@ -122,6 +122,31 @@ dense_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan
     }
 }
 
+// The dense trailing blocks with a 2-CTA thread-block cluster per system
+// (the two CTAs split the trailing updates): rank 0 draws a system, both
+// read it through distributed shared memory between two cluster barriers.
+template <typename VT>
+__global__ void __launch_bounds__(512, 1)
+dense_cluster_kernel(const SysDev* __restrict__ sys, int nsys, int* queue, SmemPlan plan, SolveParams prm,
+                     const int* dyn, const int* list) {
+    extern __shared__ __align__(16) char smem[];
+    __shared__ int s_task;
+    const int ns = item_count(nsys, dyn);
+    namespace cgr = cooperative_groups;
+    cgr::cluster_group cl = cgr::this_cluster();
+    const volatile int* task0 = cl.map_shared_rank(&s_task, 0);
+    while (true) {
+        cl.sync();
+        if (cl.block_rank() == 0 && threadIdx.x == 0) s_task = atomicAdd(queue + 2, 1);
+        cl.sync();
+        const int t = *task0;
+        cl.sync();
+        if (t >= ns) break;
+        const SysDev S = sys[list ? list[t] : t];
+        dense_phase<VT, true>(S, plan, smem, prm);
+    }
+}
+
 // After the solve of one system (thread 0, past the CTA barrier that makes
 // the solve's statistics visible): record the rung that produced the
 // result and hand a failed system to the next rung of the ladder.
@@ -643,10 +668,32 @@ static int refactor_cluster_count(size_t smem, int block, int csize, int* nclust
 }
 
 template <typename VT>
-static int dense_prepare(size_t smem, int block, int* occ) {
+static int dense_prepare(size_t smem, int block, int* occ, bool cluster = false) {
     static std::mutex mu;
-    static size_t granted = 0;
-    return prepare_kernel(dense_kernel<VT>, smem, block, occ, &granted, mu);
+    static size_t granted[2] = {0, 0};
+    if (cluster) return prepare_kernel(dense_cluster_kernel<VT>, smem, block, occ, &granted[1], mu);
+    return prepare_kernel(dense_kernel<VT>, smem, block, occ, &granted[0], mu);
+}
+
+// 2-CTA clusters of the dense-block kernel that can be resident at once.
+template <typename VT>
+static int dense_cluster_count(size_t smem, int block, int* nclusters) {
+    int rc = dense_prepare<VT>(smem, block, nullptr, true);
+    if (rc != LUSP_OK) return rc;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2u * sm_count());
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(nclusters, dense_cluster_kernel<VT>, &cfg);
+    if (e != cudaSuccess) return cuda_fail(e, "dense cluster occupancy query");
+    return LUSP_OK;
 }
 
 // Loads every kernel of the engine into the current context (CUDA loads a
@@ -659,6 +706,7 @@ int preload_kernels() {
         (const void*)refactor_fn<double>(768), (const void*)refactor_fn<float>(768, true),
         (const void*)refactor_fn<float>(512, true), (const void*)refactor_fn<double>(768, true),
         (const void*)refactor_fn<double>(512, true), (const void*)dense_kernel<float>, (const void*)dense_kernel<double>,
+        (const void*)dense_cluster_kernel<float>, (const void*)dense_cluster_kernel<double>,
         (const void*)solve_kernel<float, float>, (const void*)solve_kernel<float, double>,
         (const void*)solve_kernel<float, __half>, (const void*)solve_kernel<double, double>};
     for (const void* f : fns) {
@@ -686,16 +734,17 @@ struct RungShape {
     SmemPlan rplan, dplan, plan;
     int rblock, rgrid, rcluster, dblock, dgrid, block, grid;
     SpreadArgs rspread;
+    int dcluster;
 };
 
 static RungShape main_shape(const LaunchArgs& a) {
     return RungShape{a.rplan, a.dplan, a.plan, a.rblock, a.rgrid, a.rcluster, a.dblock, a.dgrid, a.block, a.grid,
-                     a.rspread};
+                     a.rspread, a.dcluster};
 }
 
 static RungShape ladder_shape(const LaunchArgs& a) {
     return RungShape{a.xrplan, a.xdplan, a.xplan, a.xrblock, a.xrgrid, a.xrcluster, a.xdblock, a.xdgrid,
-                     a.xblock, a.xgrid, a.xrspread};
+                     a.xblock, a.xgrid, a.xrspread, 1};
 }
 
 // Refactor, dense-block and solve kernels of one rung over sys[0, nsys) (or
@@ -742,10 +791,26 @@ static int launch_rung(const SysDev* sys, int nsys, int* q, const int* dyn, cons
         if (e != cudaSuccess) return cuda_fail(e, "refactor kernel launch");
         if (kev && cudaEventRecord(kev[1], st) != cudaSuccess) return cuda_fail(cudaGetLastError(), "timing event");
         if (r.dgrid > 0) {
-            rc = dense_prepare<VT>(r.dplan.bytes, r.dblock, nullptr);
+            rc = dense_prepare<VT>(r.dplan.bytes, r.dblock, nullptr, r.dcluster > 1);
             if (rc != LUSP_OK) return rc;
-            dense_kernel<VT><<<r.dgrid, r.dblock, r.dplan.bytes, st>>>(sys, nsys, q, r.dplan, prm, dyn, list);
-            e = cudaGetLastError();
+            if (r.dcluster > 1) {
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)r.dgrid);
+                cfg.blockDim = dim3((unsigned)r.dblock);
+                cfg.dynamicSmemBytes = r.dplan.bytes;
+                cfg.stream = st;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = 2;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                e = cudaLaunchKernelEx(&cfg, dense_cluster_kernel<VT>, sys, nsys, q, r.dplan, prm, dyn, list);
+            } else {
+                dense_kernel<VT><<<r.dgrid, r.dblock, r.dplan.bytes, st>>>(sys, nsys, q, r.dplan, prm, dyn, list);
+                e = cudaGetLastError();
+            }
             if (e != cudaSuccess) return cuda_fail(e, "dense kernel launch");
         }
     } else if (kev && cudaEventRecord(kev[1], st) != cudaSuccess) {
@@ -989,6 +1054,19 @@ int refactor_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& 
         if (rc != LUSP_OK) return rc;
         if (docc < 1) { set_error("dense kernel does not fit one SM (smem %zu)", a.dplan.bytes); return LUSP_EARG; }
         a.dgrid = std::min(ntail, docc * sm_count());
+        // Two CTAs per block (a 2-CTA cluster that splits the trailing
+        // updates) when every system with a block gets its pair of SMs.
+        a.dcluster = 1;
+        if (a.dplan.tnb == 32 && 2 * ntail <= sm_count()) {
+            int ncl = 0;
+            rc = o.prec == LUSP_FP64 ? dense_cluster_count<double>(a.dplan.bytes, a.dblock, &ncl)
+                                     : dense_cluster_count<float>(a.dplan.bytes, a.dblock, &ncl);
+            if (rc != LUSP_OK) return rc;
+            if (ncl >= ntail) {
+                a.dcluster = 2;
+                a.dgrid = 2 * ntail;
+            }
+        }
     }
     return LUSP_OK;
 }
@@ -1027,7 +1105,7 @@ int ladder_setup(const std::vector<PatternObj*>& pats, const lusp_batch_opts& o,
     a.xrcluster = r.rcluster;
     a.xdplan = r.dplan;
     a.xdblock = r.dblock;
-    a.xdgrid = r.dgrid;
+    a.xdgrid = r.dcluster > 1 ? r.dgrid / r.dcluster : r.dgrid;   // the ladder's dense kernel runs lone CTAs
     fill_params(a.xprm, x);
     a.xprm.shift = 0.0;
     a.hard_shift = o.hard_shift > 0 ? o.hard_shift : 1e-7;

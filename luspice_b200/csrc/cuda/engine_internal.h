@@ -45,6 +45,7 @@ struct LaunchArgs {
     SmemPlan dplan{};                // dense trailing-block kernel (dgrid 0: none)
     int dblock = 512;
     int dgrid = 0;
+    int dcluster = 1;                // CTAs per system of the dense-block kernel (cluster)
     // Escalation ladder after a mixed solve (rungs: bit 0 P-safe, bit 1
     // P-hard; 0 none): fp64 kernels over the slots the solve kernel takes.
     int rungs = 0;

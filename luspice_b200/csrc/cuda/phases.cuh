@@ -149,16 +149,32 @@ __device__ void cta_store_pivot_stats(SysStats* st, Smem& sm, double minpiv, dou
 // Entry (r, c) of the dense trailing block W, or 0 when it is outside the
 // block's pattern (first panel step only: the refactor wrote the pattern
 // entries alone, the rest of W holds whatever an earlier launch left).
+// Split thread-block cluster barrier (every thread of both CTAs arrives,
+// then waits; release / acquire at cluster scope).
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+
+template <bool CG = false>
 __device__ __forceinline__ double tail_entry(const double* W, int ld, const unsigned* mask, int r, int c,
                                              bool masked) {
     if (masked && !((__ldg(mask + (size_t)r * (ld >> 5) + (c >> 5)) >> (c & 31)) & 1u)) return 0.0;
-    return W[(size_t)r * ld + c];
+    return CG ? __ldcg(W + (size_t)r * ld + c) : W[(size_t)r * ld + c];
 }
 
-template <typename VT>
+// CL: the block is shared by the two CTAs of a thread-block cluster.  Rank
+// 0 factors each panel alone, one step ahead (look-ahead); rank 1 copies it
+// from rank 0's shared memory.  In each step rank 0 takes the U rows and the
+// trailing update of the next panel's columns, rank 1 those of all other
+// columns, so each column of W is written by one CTA between two cluster
+// barriers.  W is then read through L2 (ld.cg), where the other CTA's writes
+// are, never from a stale L1 line.
+template <typename VT, bool CL = false>
 __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, const SmemPlan& plan,
                                   const SolveParams& prm, double& minpiv, double& minratio, int& bad,
                                   SysStats* st) {
+    namespace cgr = cooperative_groups;
+    const int crank = CL ? (int)cgr::this_cluster().block_rank() : 0, csize = CL ? 2 : 1;
+    const bool lead = crank == 0;
     const int D = P.dtail, ld = P.tail_ld, k0 = P.k0, nb = plan.tnb;
     const int ps = nb + 1;   // panel row stride: odd, so a lane per row hits distinct banks
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
@@ -174,18 +190,21 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
         ctr[3] = clock64();
     }
     const unsigned* mask = P.tail_mask;
-    for (int jb = 0; jb < D; jb += nb) {
+    auto wld = [W](size_t i) { return CL ? __ldcg(W + i) : W[i]; };
+    const int warp = tid >> 5, nw = nt >> 5;
+    // Panel jb: loaded into shared memory, factored, its pivot statistics
+    // taken and written back to W (rank 0 alone in a cluster).
+    auto panel = [&](int jb) {
         const int w = min(nb, D - jb), R = D - jb;
         const bool first = jb == 0;
         for (int t = tid; t < R * nb; t += nt) {
             const int r = t / nb, c = t - r * nb;
-            pan[r * ps + c] = c < w ? tail_entry(W, ld, mask, jb + r, jb + c, first) : 0.0;
+            pan[r * ps + c] = c < w ? tail_entry<CL>(W, ld, mask, jb + r, jb + c, first) : 0.0;
         }
         __syncthreads();
         // Panel: unblocked elimination, a lane per row and a warp per 32
         // rows, so a row's multiplier and its update stay inside one warp:
         // one CTA barrier per column (the pivot row must be final for all).
-        const int warp = tid >> 5, nw = nt >> 5;
         for (int c = 0; c < w; c++) {
             const double piv = pan[c * ps + c];
             const double* urow = pan + (size_t)c * ps;
@@ -237,26 +256,66 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
             if (c < w) W[(size_t)(jb + r) * ld + jb + c] = pan[r * ps + c];
         }
         __syncthreads();
+    };
+    // A cluster factors panel 0 before the loop and each later panel one
+    // step ahead: rank 0 owns the next panel's 32 columns in the trailing
+    // update of the current step and factors that panel right after them,
+    // while rank 1 updates every other column (so the panel chain overlaps
+    // the bulk of the update).
+    if (CL && lead) panel(0);
+    for (int jb = 0; jb < D; jb += nb) {
+        const int w = min(nb, D - jb), R = D - jb;
+        const bool first = jb == 0;
+        if (!CL) panel(jb);
+        if (CL) {
+            // The panel is final in rank 0's shared memory and in W (first
+            // cluster barrier); rank 1 copies its multipliers, and rank 0
+            // overwrites them with the next panel only after the second
+            // (split: rank 0 arrives at once and waits just before that).
+            cluster_arrive();
+            cluster_wait();
+            if (!lead) {
+                const double* pan0 = cgr::this_cluster().map_shared_rank(pan, 0);
+                for (int t = tid; t < R * ps; t += nt) pan[t] = pan0[t];
+            }
+            cluster_arrive();
+            if (!lead) {
+                cluster_wait();
+                __syncthreads();
+            }
+        }
         if (tid == 0) {
             const long long t2 = clock64();
             ctr[0] += t2 - ctr[3];
             ctr[3] = t2;
         }
         const int c1 = jb + w, ncols = D - c1;
-        if (ncols <= 0) break;
+        if (ncols <= 0) {
+            if (CL && lead) cluster_wait();
+            break;
+        }
+        // This CTA's columns of the trailing part, colof(t) the t-th: all of
+        // them, or (CL) the next panel's nb columns for rank 0 and the rest
+        // for rank 1.
+        const int cown = CL && !lead ? c1 + nb : c1;
+        const int nown = CL ? (lead ? min(nb, ncols) : max(0, ncols - nb)) : ncols;
+        const int cend = cown + nown;   // this CTA's columns: [cown, cend)
+        auto colof = [&](int t) { return cown + t; };
         // U rows of the panel (triangular solve with the unit-L diagonal
         // block), one thread per column, in groups of 8 rows so the column
         // stays in registers.
-        for (int t = tid; t < ncols; t += nt) {
-            const size_t col = (size_t)c1 + t;
+        for (int t = tid; t < nown; t += nt) {
+            const int colc = colof(t);
+            if (colc >= cend) continue;
+            const size_t col = (size_t)colc;
             for (int g = 0; g < w; g += 8) {
                 double u[8];
 #pragma unroll
-                for (int r = 0; r < 8; r++) u[r] = g + r < w ? tail_entry(W, ld, mask, jb + g + r, (int)col, first) : 0.0;
+                for (int r = 0; r < 8; r++) u[r] = g + r < w ? tail_entry<CL>(W, ld, mask, jb + g + r, (int)col, first) : 0.0;
                 for (int g2 = 0; g2 < g; g2 += 8) {
                     double v[8];
 #pragma unroll
-                    for (int c = 0; c < 8; c++) v[c] = W[(size_t)(jb + g2 + c) * ld + col];
+                    for (int c = 0; c < 8; c++) v[c] = wld((size_t)(jb + g2 + c) * ld + col);
 #pragma unroll
                     for (int c = 0; c < 8; c++)
 #pragma unroll
@@ -284,12 +343,13 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
         // columns (lane + 32 j); multipliers from the panel in shared memory
         // (broadcast within a warp), U12 staged per tile.
         const int TR = 4 * nw;
-        const int nrt = (ncols + TR - 1) / TR, nct = (ncols + 127) / 128;
+        const int nrt = (ncols + TR - 1) / TR, nct = (nown + 127) / 128;
         for (int tile = 0; tile < nrt * nct; tile++) {
-            const int r0 = c1 + (tile / nct) * TR, q0 = c1 + (tile % nct) * 128;
+            const int r0 = c1 + (tile / nct) * TR, tq = (tile % nct) * 128;
             for (int t = tid; t < w * 128; t += nt) {
                 const int c = t >> 7, x = t & 127;
-                ut[t] = q0 + x < D ? W[(size_t)(jb + c) * ld + q0 + x] : 0.0;
+                const int col = colof(tq + x);
+                ut[t] = col < cend ? wld((size_t)(jb + c) * ld + col) : 0.0;
             }
             __syncthreads();
             const int rw = r0 + warp;
@@ -302,8 +362,8 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
                     lo[q] = row < D ? q * nw * ps : 0;   // rows past the block reuse rw's multipliers
 #pragma unroll
                     for (int j = 0; j < 4; j++) {
-                        const int col = q0 + lane + 32 * j;
-                        acc[q][j] = (row < D && col < D) ? tail_entry(W, ld, mask, row, col, first) : 0.0;
+                        const int col = colof(tq + lane + 32 * j);
+                        acc[q][j] = (row < D && col < cend) ? tail_entry<CL>(W, ld, mask, row, col, first) : 0.0;
                     }
                 }
                 const double* l0 = pan + (size_t)(rw - jb) * ps;
@@ -323,8 +383,8 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
                     const int row = rw + q * nw;
 #pragma unroll
                     for (int j = 0; j < 4; j++) {
-                        const int col = q0 + lane + 32 * j;
-                        if (row < D && col < D) W[(size_t)row * ld + col] = acc[q][j];
+                        const int col = colof(tq + lane + 32 * j);
+                        if (row < D && col < cend) W[(size_t)row * ld + col] = acc[q][j];
                     }
                 }
             }
@@ -334,6 +394,20 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
             const long long t2 = clock64();
             ctr[2] += t2 - ctr[3];
             ctr[3] = t2;
+        }
+        if (CL && lead) {
+            // The next panel's columns are final (this CTA's own update):
+            // make them visible at L2, where the panel load reads; rank 1
+            // is done copying this panel.
+            __threadfence();
+            __syncthreads();
+            cluster_wait();
+            panel(c1);
+            if (tid == 0) {
+                const long long t2 = clock64();
+                ctr[0] += t2 - ctr[3];
+                ctr[3] = t2;
+            }
         }
     }
     if (tid == 0) {
@@ -346,7 +420,7 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
 // Dense trailing block -> VT storage for the solves (unit L below the
 // diagonal, U on and above).  The block's entries live only there (the
 // merged slot array gets them from merge_factor_kernel when a caller asks).
-template <typename VT>
+template <typename VT, bool CG = false>
 __device__ void dense_tail_store(const SysDev& S, const PatternDev& P, const double* W, double& maxu,
                                  char* smem_tail_tiles, int ttw) {
     const int D = P.dtail, ld = P.tail_ld, k0 = P.k0;
@@ -366,7 +440,7 @@ __device__ void dense_tail_store(const SysDev& S, const PatternDev& P, const dou
                     const int i = ti * 32 + r, c = tc * 32 + lane;
                     double v = 0.0;
                     if (i < D && c < D) {
-                        v = W[(size_t)i * ld + c];
+                        v = CG ? __ldcg(W + (size_t)i * ld + c) : W[(size_t)i * ld + c];
                         if (i <= c) maxu = fmax(maxu, fabs(v));
                     }
                     tile[r * 33 + lane] = v;
@@ -384,7 +458,9 @@ __device__ void dense_tail_store(const SysDev& S, const PatternDev& P, const dou
 
 // The dense trailing block of one system (its own kernel: few warps, many
 // registers each): factor, store, merge the pivot statistics.
-template <typename VT>
+// CL: the two CTAs of a thread-block cluster share the system (see
+// dense_tail_factor); rank 0 stores the factor and the statistics.
+template <typename VT, bool CL = false>
 __device__ void dense_phase(const SysDev& S, const SmemPlan& plan, char* smem_base, const SolveParams& prm) {
     const PatternDev& P = *S.pat;
     if (P.dtail <= 0) return;
@@ -396,9 +472,10 @@ __device__ void dense_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
     __syncthreads();
     double minpiv = INFINITY, minratio = INFINITY, maxu = 0.0;
     int bad = 0;
-    dense_tail_factor<VT>(P, S.tailw, sm, plan, prm, minpiv, minratio, bad, S.stats);
+    dense_tail_factor<VT, CL>(P, S.tailw, sm, plan, prm, minpiv, minratio, bad, S.stats);
     __syncthreads();
-    dense_tail_store<VT>(S, P, S.tailw, maxu, sm.uni, plan.ttw);
+    if (CL && cooperative_groups::this_cluster().block_rank() != 0) return;
+    dense_tail_store<VT, CL>(S, P, S.tailw, maxu, sm.uni, plan.ttw);
     cta_store_pivot_stats(S.stats, sm, minpiv, minratio, maxu, bad, false, sm.ctl);
 }
 
