@@ -342,8 +342,45 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
         // columns: a thread owns four rows (one per warp stride) and four
         // columns (lane + 32 j); multipliers from the panel in shared memory
         // (broadcast within a warp), U12 staged per tile.
+        if (CL && lead) {
+            // Rank 0's single panel-wide chunk (at most 32 columns): tiles
+            // of 16 nw rows x 32 columns, a thread owning one column and 16
+            // rows (one per warp stride), so no lane idles.
+            const int TRn = 16 * nw;
+            for (int r0 = c1; r0 < D; r0 += TRn) {
+                for (int t = tid; t < w * 32; t += nt) {
+                    const int c = t >> 5, x = t & 31;
+                    const int col = cown + x;
+                    ut[c * 128 + x] = col < cend ? wld((size_t)(jb + c) * ld + col) : 0.0;
+                }
+                __syncthreads();
+                const int rw = r0 + warp, col = cown + lane;
+                if (rw < D) {
+                    double acc[16];
+                    int lo[16];
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        const int row = rw + k * nw;
+                        lo[k] = row < D ? k * nw * ps : 0;   // rows past the block reuse rw's multipliers
+                        acc[k] = (row < D && col < cend) ? tail_entry<CL>(W, ld, mask, row, col, first) : 0.0;
+                    }
+                    const double* l0 = pan + (size_t)(rw - jb) * ps;
+                    for (int c = 0; c < w; c++) {
+                        const double u = ut[c * 128 + lane];
+#pragma unroll
+                        for (int k = 0; k < 16; k++) acc[k] = __dsub_rn(acc[k], __dmul_rn(l0[lo[k] + c], u));
+                    }
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        const int row = rw + k * nw;
+                        if (row < D && col < cend) W[(size_t)row * ld + col] = acc[k];
+                    }
+                }
+                __syncthreads();
+            }
+        }
         const int TR = 4 * nw;
-        const int nrt = (ncols + TR - 1) / TR, nct = (nown + 127) / 128;
+        const int nrt = (ncols + TR - 1) / TR, nct = CL && lead ? 0 : (nown + 127) / 128;
         for (int tile = 0; tile < nrt * nct; tile++) {
             const int r0 = c1 + (tile / nct) * TR, tq = (tile % nct) * 128;
             for (int t = tid; t < w * 128; t += nt) {
@@ -410,7 +447,7 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
             }
         }
     }
-    if (tid == 0) {
+    if (tid == 0 && lead) {
         st->cyc_tpanel = ctr[0];
         st->cyc_ttrsm = ctr[1];
         st->cyc_tupdate = ctr[2];
