@@ -1208,6 +1208,51 @@ __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.w
 // UPPER: y[i] = (y[i] - sum) / diag (U sweep), else y[i] -= sum.
 constexpr int kStages = 4;
 
+// Bulk asynchronous copies (TMA, untiled) with completion on an mbarrier in
+// shared memory: 16-byte aligned addresses, sizes a multiple of 16 bytes.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(unsigned long long* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+// The barriers' initialization, visible to the asynchronous proxy.
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+// Earlier generic-proxy accesses to shared memory ordered before later
+// asynchronous-proxy (bulk copy) writes.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for phase `parity` of bar: false (and the status bit set)
+// when it does not complete within kSpinLimit polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int* status) {
+    for (long long it = 0; !mbar_try_wait(bar, parity); it++) {
+        if (it > kSpinLimit) {
+            if (status) atomicOr(status, ST_WAIT_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
+
 // sum over e = e0, e0 + g, ... < pe of val[e] * y[col[e]]: four partial
 // sums, so a lane has four loads of y in flight when y lives in global
 // memory (a row with fewer than four entries per lane keeps one sum).
@@ -1245,7 +1290,7 @@ __device__ __forceinline__ void sweep_barrier(int nthreads) {
 template <typename VT, bool UPPER, bool GY>
 __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* lgl, const int* order, const int* rp,
                              const int* ci, const VT* val, const VT* dgo, double* y,
-                             char* stage, int cap_e, int cap_r, double* part) {
+                             char* stage, int cap_e, int cap_r, double* part, int* status) {
     const int NT = min((int)blockDim.x, kSweepThreads);
     if ((int)threadIdx.x >= NT) {
         __syncthreads();
@@ -1256,39 +1301,47 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
     const int warp = threadIdx.x >> 5;
     const bool pow2 = (NT & (NT - 1)) == 0;
     const int lgb = 31 - __clz(NT);
-    // The copies are issued from the highest threads down: rows go to the
-    // lowest warps, so in a narrow level the warps that issue are not the
-    // ones that compute (issuing a level's copies takes a warp ~500 cycles,
-    // which sat on the critical warp 0 of every level).
-    const int itid = NT - 1 - (int)threadIdx.x;
+    // Each staged level is three bulk copies (column indices, values and,
+    // for U, the reciprocal diagonal: contiguous runs in sweep order, rounded
+    // out to 16-byte boundaries; every array has slack past its end for the
+    // rounding) issued by one thread, the last one (rows go to the lowest
+    // warps), completing on the slot's mbarrier; every thread waits on that
+    // barrier's phase before the level's CTA barrier.
+    __shared__ unsigned long long mbar[kStages];
+    const bool issuer = (int)threadIdx.x == NT - 1;
+    auto staged = [&](const int4& d) { return d.w - d.z <= cap_e && d.y - d.x <= cap_r; };
+    // Every level arrives on its slot's barrier (a level too large for a
+    // stage with no bytes), so the k-th use of a slot is its phase k.
     auto issue = [&](int L) {
-        if (L < nlev) {
-            const int4 d = ld4[L];
-            if (d.w - d.z <= cap_e && d.y - d.x <= cap_r) {
-                char* base = stage + (size_t)(L % kStages) * sb;
-                int* sc = (int*)base;
-                VT* sv = (VT*)(base + (size_t)CE * 4);
-                VT* sd = (VT*)(base + (size_t)CE * (4 + sizeof(VT)));
-                const int a0 = d.z & ~3, n4 = ((d.w + 3) & ~3) - a0;
-                for (int t = itid * 4; t < n4; t += NT * 4) {
-                    cp_async_16(sc + t, ci + a0 + t);
-                    cp_async_16(sv + t, val + a0 + t);
-                    if (sizeof(VT) == 8) cp_async_16(sv + t + 2, val + a0 + t + 2);
-                }
-                if (UPPER) {
-                    const int b0 = d.x & ~3, m4 = ((d.y + 3) & ~3) - b0;
-                    for (int t = itid * 4; t < m4; t += NT * 4) {
-                        cp_async_16(sd + t, dgo + b0 + t);
-                        if (sizeof(VT) == 8) cp_async_16(sd + t + 2, dgo + b0 + t + 2);
-                    }
-                }
-            }
+        if (!issuer || L >= nlev) return;
+        const int4 d = ld4[L];
+        if (!staged(d)) {
+            mbar_expect_tx(&mbar[L % kStages], 0u);
+            return;
         }
-        cp_async_commit();
+        char* base = stage + (size_t)(L % kStages) * sb;
+        int* sc = (int*)base;
+        VT* sv = (VT*)(base + (size_t)CE * 4);
+        VT* sd = (VT*)(base + (size_t)CE * (4 + sizeof(VT)));
+        const int a0 = d.z & ~3, n4 = ((d.w + 3) & ~3) - a0;
+        const int b0 = d.x & ~3, m4 = UPPER ? ((d.y + 3) & ~3) - b0 : 0;
+        unsigned long long* bar = &mbar[L % kStages];
+        fence_proxy_async();
+        mbar_expect_tx(bar, (unsigned)((size_t)n4 * (4 + sizeof(VT)) + (size_t)m4 * sizeof(VT)));
+        if (n4 > 0) {
+            bulk_g2s(sc, ci + a0, (unsigned)n4 * 4u, bar);
+            bulk_g2s(sv, val + a0, (unsigned)(n4 * sizeof(VT)), bar);
+        }
+        if (UPPER && m4 > 0) bulk_g2s(sd, dgo + b0, (unsigned)(m4 * sizeof(VT)), bar);
     };
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kStages; k++) mbar_init(&mbar[k], 1);
+        fence_mbar_init();
+    }
+    sweep_barrier(NT);
     for (int L = 0; L < kStages - 1; L++) issue(L);
     for (int L = 0; L < nlev; L++) {
-        cp_async_wait_group<kStages - 2>();
+        mbar_wait(&mbar[L % kStages], (unsigned)(L / kStages) & 1u, status);
         sweep_barrier(NT);
         issue(L + kStages - 1);
         const int4 d = ld4[L];
@@ -1394,7 +1447,10 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
             if (r < r1 && lig == 0) y[i] = UPPER ? (yi - acc) * di : yi - acc;
         }
     }
-    cp_async_wait_all();
+    // Every staged level's copies were waited for; the barriers are free.
+    sweep_barrier(NT);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < kStages; k++) mbar_inval(&mbar[k]);
     __syncthreads();
 }
 
@@ -1491,10 +1547,10 @@ __device__ void cta_lu_apply_levels(const SysDev& S, const PatternDev& P, const 
     const bool gy = P.n > plan.ycap;
     if (gy)
         staged_sweep<VT, false, true>(P.nfwd_levels, sd.f_ld, sd.f_lg, sd.f_ord, sd.f_rp, P.lci, (const VT*)S.lval,
-                                      nullptr, y, stage, plan.sc_ent, plan.sc_rows, part);
+                                      nullptr, y, stage, plan.sc_ent, plan.sc_rows, part, &S.stats->status);
     else
         staged_sweep<VT, false, false>(P.nfwd_levels, sd.f_ld, sd.f_lg, sd.f_ord, sd.f_rp, P.lci,
-                                       (const VT*)S.lval, nullptr, y, stage, plan.sc_ent, plan.sc_rows, part);
+                                       (const VT*)S.lval, nullptr, y, stage, plan.sc_ent, plan.sc_rows, part, &S.stats->status);
     const long long t1 = clock64();
     if (P.dtail > 0) {
         tail_forward<VT>(P, (const VT*)S.tail, y, S.stats);
@@ -1503,10 +1559,10 @@ __device__ void cta_lu_apply_levels(const SysDev& S, const PatternDev& P, const 
     const long long t2 = clock64();
     if (gy)
         staged_sweep<VT, true, true>(P.nbwd_levels, sd.b_ld, sd.b_lg, sd.b_ord, sd.b_rp, P.uci, (const VT*)S.uval,
-                                     (const VT*)S.udiag_bwd, y, stage, plan.sc_ent, plan.sc_rows, part);
+                                     (const VT*)S.udiag_bwd, y, stage, plan.sc_ent, plan.sc_rows, part, &S.stats->status);
     else
         staged_sweep<VT, true, false>(P.nbwd_levels, sd.b_ld, sd.b_lg, sd.b_ord, sd.b_rp, P.uci, (const VT*)S.uval,
-                                      (const VT*)S.udiag_bwd, y, stage, plan.sc_ent, plan.sc_rows, part);
+                                      (const VT*)S.udiag_bwd, y, stage, plan.sc_ent, plan.sc_rows, part, &S.stats->status);
     if (threadIdx.x == 0) {
         S.stats->cyc_lsolve += t1 - t0;
         S.stats->cyc_tail += t2 - t1;
