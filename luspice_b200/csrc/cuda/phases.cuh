@@ -1283,6 +1283,52 @@ __device__ __forceinline__ void sweep_barrier(int nthreads) {
     asm volatile("bar.sync 1, %0;\n" ::"r"(nthreads) : "memory");
 }
 
+// The rows [r0, r1) of one level, 2^LG lanes per row (a compile-time group
+// width, so the row reduction is unrolled), in rounds of NT / 2^LG rows.
+template <typename VT, bool UPPER, bool GY, int LG>
+__device__ __forceinline__ void sweep_rows(int r0, int r1, int NT, const int* order, const int* rp, const int* cc,
+                                           const VT* vv, const VT* dd, int eb, int rb, double* y) {
+    constexpr int g = 1 << LG;
+    const int lig = threadIdx.x & (g - 1);
+    const int warp = threadIdx.x >> 5;
+    const int ngr = NT >> LG;
+    for (int rbase = r0; rbase < r1; rbase += ngr) {
+        if (rbase + ((warp * 32) >> LG) >= r1) break;   // nothing left for this warp
+        const int r = rbase + ((int)threadIdx.x >> LG);
+        double acc = 0.0, yi = 0.0, di = 1.0;
+        int i = 0;
+        if (r < r1) {
+            // The row's own right-hand side and diagonal, loaded beside the
+            // dot product instead of after its reduction (no other thread
+            // writes y[i] in this level).
+            if (lig == 0) {
+                i = order[r];
+                yi = y[i];
+                if (UPPER) di = ValTraits<VT>::load(dd + (r - rb));
+            }
+            if (GY) {
+                acc = row_dot<VT>(vv, cc, y, rp[r] - eb + lig, rp[r + 1] - eb, g);
+            } else {
+                // Two entries per lane in flight.
+                const int pe = rp[r + 1] - eb;
+                int e = rp[r] - eb + lig;
+                double a1 = 0.0;
+                for (; e + g < pe; e += 2 * g) {
+                    const int c0 = cc[e], c1 = cc[e + g];
+                    const double v0 = ValTraits<VT>::load(vv + e), v1 = ValTraits<VT>::load(vv + e + g);
+                    acc = fma(v0, y[c0], acc);
+                    a1 = fma(v1, y[c1], a1);
+                }
+                if (e < pe) acc = fma(ValTraits<VT>::load(vv + e), y[cc[e]], acc);
+                acc += a1;
+            }
+        }
+#pragma unroll
+        for (int o = g >> 1; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, g);
+        if (r < r1 && lig == 0) y[i] = UPPER ? (yi - acc) * di : yi - acc;
+    }
+}
+
 // GY: y lives in global memory (large systems): levels of a few long rows
 // (64 entries or more on average) get several warps per row, and long rows
 // four partial sums per lane; with y in shared memory a lane keeps one sum
@@ -1299,8 +1345,6 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
     const int CE = cap_e + 8;
     const size_t sb = stage_bytes(cap_e, cap_r, sizeof(VT));
     const int warp = threadIdx.x >> 5;
-    const bool pow2 = (NT & (NT - 1)) == 0;
-    const int lgb = 31 - __clz(NT);
     // Each staged level is three bulk copies (column indices, values and,
     // for U, the reciprocal diagonal: contiguous runs in sweep order, rounded
     // out to 16-byte boundaries; every array has slack past its end for the
@@ -1407,44 +1451,13 @@ __device__ __noinline__ void staged_sweep(int nlev, const int4* ld4, const int* 
                 continue;
             }
         }
-        const int lg = min(lgd, 5), g = 1 << lg;
-        const int lig = threadIdx.x & (g - 1);
-        const int ngr = NT >> lg;
-        const int rounds = pow2 ? (nr + ngr - 1) >> (lgb - lg) : (nr + ngr - 1) / ngr;
-        for (int rd = 0; rd < rounds; rd++) {
-            const int rbase = r0 + rd * ngr;
-            if (rbase + ((warp * 32) >> lg) >= r1) break;   // nothing left for this warp
-            const int r = rbase + ((int)threadIdx.x >> lg);
-            double acc = 0.0, yi = 0.0, di = 1.0;
-            int i = 0;
-            if (r < r1) {
-                // The row's own right-hand side and diagonal, loaded beside
-                // the dot product instead of after its reduction (no other
-                // thread writes y[i] in this level).
-                if (lig == 0) {
-                    i = order[r];
-                    yi = y[i];
-                    if (UPPER) di = ValTraits<VT>::load(dd + (r - rb));
-                }
-                if (GY) {
-                    acc = row_dot<VT>(vv, cc, y, rp[r] - eb + lig, rp[r + 1] - eb, g);
-                } else {
-                    // Two entries per lane in flight.
-                    const int pe = rp[r + 1] - eb;
-                    int e = rp[r] - eb + lig;
-                    double a1 = 0.0;
-                    for (; e + g < pe; e += 2 * g) {
-                        const int c0 = cc[e], c1 = cc[e + g];
-                        const double v0 = ValTraits<VT>::load(vv + e), v1 = ValTraits<VT>::load(vv + e + g);
-                        acc = fma(v0, y[c0], acc);
-                        a1 = fma(v1, y[c1], a1);
-                    }
-                    if (e < pe) acc = fma(ValTraits<VT>::load(vv + e), y[cc[e]], acc);
-                    acc += a1;
-                }
-            }
-            for (int o = g >> 1; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, g);
-            if (r < r1 && lig == 0) y[i] = UPPER ? (yi - acc) * di : yi - acc;
+        switch (min(lgd, 5)) {
+            case 0: sweep_rows<VT, UPPER, GY, 0>(r0, r1, NT, order, rp, cc, vv, dd, eb, rb, y); break;
+            case 1: sweep_rows<VT, UPPER, GY, 1>(r0, r1, NT, order, rp, cc, vv, dd, eb, rb, y); break;
+            case 2: sweep_rows<VT, UPPER, GY, 2>(r0, r1, NT, order, rp, cc, vv, dd, eb, rb, y); break;
+            case 3: sweep_rows<VT, UPPER, GY, 3>(r0, r1, NT, order, rp, cc, vv, dd, eb, rb, y); break;
+            case 4: sweep_rows<VT, UPPER, GY, 4>(r0, r1, NT, order, rp, cc, vv, dd, eb, rb, y); break;
+            default: sweep_rows<VT, UPPER, GY, 5>(r0, r1, NT, order, rp, cc, vv, dd, eb, rb, y); break;
         }
     }
     // Every staged level's copies were waited for; the barriers are free.
