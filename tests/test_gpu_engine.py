@@ -238,3 +238,38 @@ def test_refactor_spread_singular_column(gpu):
         B.close()
     assert sts[5]["status"] & api.ST_SINGULAR
     assert sts[5]["singular_col"] == sts[-1]["singular_col"] >= 0
+
+
+def test_launch_shapes_same_factor(gpu):
+    """The launch rules pick spread mode (up to 12 CTAs of 256 threads per
+    system, global-memory sync) for medium systems and a 2-CTA cluster for
+    the dense trailing block; the factor bits, statistics and solutions are
+    the same under every shape (spread, 2-CTA cluster refactor, lone CTAs),
+    and equal the host restatement."""
+    m = mna.power_grid()
+    P = api.Pattern.from_matrix(m)
+    vals = m.perturbed(4, seed=77)
+    shapes = [dict(), dict(refactor_cluster=2), dict(refactor_cluster=1, refactor_threads=768),
+              dict(refactor_spread=5, refactor_threads=512)]
+    res = []
+    for opts in shapes:
+        B = api.Batch([P] * 4, prec=api.MIXED, **opts)
+        B.upload(list(vals), [m.b] * 4)
+        B.run(api.RUN_BOTH)
+        sh = B.launch_shape()
+        res.append((sh, [B.factor_values(s) for s in range(4)], B.stats(), B.split(B.download())))
+        B.close()
+    sh0 = res[0][0]
+    assert sh0["refactor_spread"] == 12 and sh0["refactor_block"] == 256, sh0
+    assert sh0["dense_cluster"] == 2 and sh0["dense_grid"] == 8, sh0
+    assert res[1][0]["refactor_cluster"] == 2 and res[1][0]["refactor_spread"] == 0, res[1][0]
+    assert res[2][0]["refactor_cluster"] == 1 and res[2][0]["refactor_spread"] == 0, res[2][0]
+    assert res[3][0]["refactor_spread"] == 5, res[3][0]
+    for s in range(4):
+        exp, bad = oracle_refactor(m, P, vals[s], fp32=True)
+        assert bad < 0
+        for k, (sh, fac, st, xs) in enumerate(res):
+            assert np.array_equal(fac[s].view(np.uint32), exp.astype(np.float32).view(np.uint32)), (k, s)
+            for key in ("min_abs_pivot", "min_pivot_ratio", "max_abs_u"):
+                assert st[s][key] == res[0][2][s][key], (k, s, key)
+            assert np.array_equal(xs[s], res[0][3][s]), (k, s)
