@@ -67,10 +67,12 @@ __device__ __forceinline__ void share_fence(unsigned csize) {
     if (csize > 1) asm volatile("fence.acq_rel.cluster;\n" ::: "memory");
     else __threadfence_block();
 }
-// GPU scope: CTAs on any SM share the system (spread mode).
+// GPU scope: CTAs on any SM share the system (spread mode).  An acq_rel
+// fence is what the release (before a ready bit) and acquire (after one)
+// patterns need; the sequentially consistent __threadfence() costs more.
 template <bool SPREAD>
 __device__ __forceinline__ void share_fence_t(unsigned csize) {
-    if (SPREAD) __threadfence();
+    if (SPREAD) asm volatile("fence.acq_rel.gpu;\n" ::: "memory");
     else share_fence(csize);
 }
 
