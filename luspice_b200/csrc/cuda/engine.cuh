@@ -115,6 +115,9 @@ struct SysDev {
                              // unit L below the diagonal
     double* tailw;           // [dtail * tail_ld] fp64 trailing block (row-major)
                              // between the refactor and dense kernels
+    void* tinv;              // [ceil(dtail/32) * 2048] inverses of the dense
+                             // block's 32 x 32 diagonal blocks (VT): per block
+                             // L^-1 then U^-1, element (i, c) at c * 32 + i
     SysStats* stats;
 };
 
@@ -148,11 +151,15 @@ __host__ __device__ inline size_t al256(size_t b) { return (b + 255) & ~(size_t)
 // dimension m.  The merged and row-major values and the sweep-order
 // diagonal get 64 bytes of slack: the kernels copy them in aligned 16-byte
 // pieces.
+__host__ __device__ inline size_t tinv_bytes(const SysSizes& z, size_t vs) {
+    return ((z.dtail + 31) / 32) * 2048 * vs;
+}
+
 __host__ __device__ inline size_t sys_private_bytes(const SysSizes& z, size_t vs, int m) {
     return al256(z.cap * vs + 64) + al256(z.nnz_l * vs + 64) + al256(z.nnz_u * vs + 64) + al256(z.n * vs) +
            al256(z.n * vs + 64) + al256(z.sell * 8) + al256(z.sell * 4) + al256((2 * (size_t)m + 8) * z.n * 8) +
            al256(z.dtail * z.tail_ld * vs) + al256(z.dtail * z.tail_ld * 8) + al256(z.sell * 2) +
-           2 * al256(z.n * 8);
+           2 * al256(z.n * 8) + al256(tinv_bytes(z, vs));
 }
 
 // Points the private arrays of D into p (sys_private_bytes of them); returns
@@ -173,6 +180,7 @@ __host__ __device__ inline char* sys_carve(SysDev& D, char* p, const SysSizes& z
     D.sell16 = p; p += al256(z.sell * 2);
     D.rs = (double*)p; p += al256(z.n * 8);
     D.cs = (double*)p; p += al256(z.n * 8);
+    D.tinv = p; p += al256(tinv_bytes(z, vs));
     return p;
 }
 

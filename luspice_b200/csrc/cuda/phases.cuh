@@ -497,6 +497,68 @@ __device__ void dense_tail_store(const SysDev& S, const PatternDev& P, const dou
 
 // The dense trailing block of one system (its own kernel: few warps, many
 // registers each): factor, store, merge the pivot statistics.
+// Inverses of the 32 x 32 diagonal blocks of the dense block's factor, for
+// the solves (a block's triangular solve becomes a matrix-vector product
+// instead of a 32-step dependent chain), from the factored fp64 block W
+// rounded to VT exactly as the stored factor is: a warp per block and
+// factor (nwork warps, each with a 32 x 33 block tile and a 32 x 33 tile of
+// the inverse at work + warp * 2 * 32 * 33 doubles), lane c computing column
+// c in fp64 by substitution; stored as VT with element (i, c) at c * 32 + i.
+// Rows and columns past a partial last block are the identity.  W read
+// through L2 (another CTA of a cluster may have written it).
+template <typename VT>
+__device__ void dense_tail_inverses(const SysDev& S, const PatternDev& P, double* work, int nwork) {
+    const int D = P.dtail, ld = P.tail_ld;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double* W = S.tailw;
+    VT* out = (VT*)S.tinv;
+    const int nbk = (D + 31) / 32;
+    double* Bs = work + (size_t)warp * 2 * 32 * 33;   // block: row r at r * 33
+    double* Xs = Bs + 32 * 33;                        // inverse: X[k][c] at k * 33 + c
+    if (warp < nwork) {
+        for (int task = warp; task < 2 * nbk; task += nwork) {
+            const int b = task >> 1, upper = task & 1, jb = b * 32, w = min(32, D - jb);
+            for (int r = 0; r < 32; r++)
+                Bs[r * 33 + lane] = (r < w && lane < w)
+                                        ? (double)ValTraits<VT>::to(__ldcg(W + (size_t)(jb + r) * ld + jb + lane))
+                                        : 0.0;
+            __syncwarp();
+            const int c = lane;
+            if (!upper) {
+                // X = L^-1 (unit lower): X[r][c] = -sum_{c<=k<r} L[r][k] X[k][c].
+                for (int r = 0; r < 32; r++) {
+                    double s0 = 0.0, s1 = 0.0;
+                    int k = 0;
+                    for (; k + 1 < r; k += 2) {
+                        s0 = fma(Bs[r * 33 + k], Xs[k * 33 + c], s0);
+                        s1 = fma(Bs[r * 33 + k + 1], Xs[(k + 1) * 33 + c], s1);
+                    }
+                    if (k < r) s0 = fma(Bs[r * 33 + k], Xs[k * 33 + c], s0);
+                    Xs[r * 33 + c] = r < c ? 0.0 : r == c ? 1.0 : r >= w ? 0.0 : -(s0 + s1);
+                    __syncwarp();
+                }
+            } else {
+                // X = U^-1: X[r][c] = -(sum_{r<k<=c} U[r][k] X[k][c]) / U[r][r].
+                for (int r = 31; r >= 0; r--) {
+                    double s0 = 0.0, s1 = 0.0;
+                    int k = r + 1;
+                    for (; k + 1 < 32; k += 2) {
+                        s0 = fma(Bs[r * 33 + k], Xs[k * 33 + c], s0);
+                        s1 = fma(Bs[r * 33 + k + 1], Xs[(k + 1) * 33 + c], s1);
+                    }
+                    if (k < 32) s0 = fma(Bs[r * 33 + k], Xs[k * 33 + c], s0);
+                    const double dg = r < w ? Bs[r * 33 + r] : 1.0;
+                    Xs[r * 33 + c] = r > c ? 0.0 : r == c ? 1.0 / dg : r >= w ? 0.0 : -(s0 + s1) / dg;
+                    __syncwarp();
+                }
+            }
+            VT* dst = out + (size_t)b * 2048 + (size_t)upper * 1024;
+            for (int cc = 0; cc < 32; cc++) dst[cc * 32 + lane] = ValTraits<VT>::to(Xs[lane * 33 + cc]);
+            __syncwarp();
+        }
+    }
+}
+
 // CL: the two CTAs of a thread-block cluster share the system (see
 // dense_tail_factor); rank 0 stores the factor and the statistics.
 template <typename VT, bool CL = false>
@@ -513,8 +575,17 @@ __device__ void dense_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
     int bad = 0;
     dense_tail_factor<VT, CL>(P, S.tailw, sm, plan, prm, minpiv, minratio, bad, S.stats);
     __syncthreads();
-    if (CL && cooperative_groups::this_cluster().block_rank() != 0) return;
+    // Warps that fit a block tile and an inverse tile in this CTA's area.
+    const size_t uoff = (size_t)(sm.uni - smem_base);
+    const int nwork = (int)min((size_t)(blockDim.x >> 5),
+                               (plan.bytes > uoff ? plan.bytes - uoff : 0) / (2 * 32 * 33 * sizeof(double)));
+    if (CL && cooperative_groups::this_cluster().block_rank() != 0) {
+        // Rank 1 computes the inverses while rank 0 stores the factor.
+        dense_tail_inverses<VT>(S, P, (double*)sm.uni, nwork);
+        return;
+    }
     dense_tail_store<VT, CL>(S, P, S.tailw, maxu, sm.uni, plan.ttw);
+    if (!CL) dense_tail_inverses<VT>(S, P, (double*)sm.uni, nwork);
     cta_store_pivot_stats(S.stats, sm, minpiv, minratio, maxu, bad, false, sm.ctl);
 }
 
@@ -1015,15 +1086,15 @@ __device__ __forceinline__ double tail_dot_regs(const VT* v, const double* y, in
 // y[k0..n) := L_tt^-1 y[k0..n) (unit lower; the tail rows' entries in the
 // columns before k0 were applied by the forward sweep's last level).
 template <typename VT>
-__device__ __noinline__ void tail_forward(const PatternDev& P, const VT* T, double* y, SysStats* st) {
+__device__ __noinline__ void tail_forward(const PatternDev& P, const VT* T, const VT* Ti, double* y, SysStats* st) {
     const int k0 = P.k0, D = P.dtail, ld = P.tail_ld;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     long long c_diag = 0, c_gemv = 0;
     double* yt = y + k0;
-    // Every thread loads one row of the block's 32 columns before the
-    // diagonal solve: warp 0 its row of the diagonal block, the other warps
-    // their first row below it (so those loads overlap the dependent chain
-    // of the diagonal solve).
+    // Every thread loads 32 values before the diagonal block: warp 0 its
+    // row of the block's inverse (L^-1, from the dense kernel), the other
+    // warps their first row of the block's 32 columns below it (so those
+    // loads overlap the diagonal product).
     const int nt = (int)blockDim.x - 32, t = (int)threadIdx.x - 32;
     for (int jb = 0; jb < D; jb += 32) {
         const int w = min(32, D - jb);
@@ -1031,14 +1102,13 @@ __device__ __noinline__ void tail_forward(const PatternDev& P, const VT* T, doub
         const int i0 = jb + w + t;
         const bool pre = t >= 0 && i0 < D;
         VT v[32];
-        if (warp == 0 || pre) tail_load_regs<VT>(T + (size_t)jb * ld + (warp == 0 ? jb + min(lane, w - 1) : i0), ld, w, v);
+        if (warp == 0) tail_load_regs<VT>(Ti + (size_t)(jb >> 5) * 2048 + lane, 32, 32, v);
+        else if (pre) tail_load_regs<VT>(T + (size_t)jb * ld + i0, ld, w, v);
         if (warp == 0) {
-            double yr = lane < w ? yt[jb + lane] : 0.0;
-#pragma unroll
-            for (int c = 0; c < 31; c++) {
-                const double yc = __shfl_sync(0xffffffffu, yr, c);
-                if (c < lane && lane < w) yr = fma(-(double)v[c], yc, yr);
-            }
+            // y_b := L_bb^-1 y_b: lane i's row of the inverse against the
+            // block of y (all lanes read it before any writes).
+            const double yr = lane < w ? tail_dot_regs<VT>(v, yt + jb, w) : 0.0;
+            __syncwarp();
             if (lane < w) yt[jb + lane] = yr;
         }
         __syncthreads();
@@ -1059,35 +1129,24 @@ __device__ __noinline__ void tail_forward(const PatternDev& P, const VT* T, doub
 
 // y[k0..n) := U_tt^-1 y[k0..n) (upper with diagonal).
 template <typename VT>
-__device__ __noinline__ void tail_backward(const PatternDev& P, const VT* T, double* y, SysStats* st) {
+__device__ __noinline__ void tail_backward(const PatternDev& P, const VT* T, const VT* Ti, double* y, SysStats* st) {
     const int k0 = P.k0, D = P.dtail, ld = P.tail_ld;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     long long c_diag = 0, c_gemv = 0;
     double* yt = y + k0;
-    // As tail_forward: warp 0 solves the diagonal block (each lane's
-    // reciprocal of its diagonal taken before the dependent chain), the
-    // other warps update the rows above it, their first row loaded before
-    // the diagonal solve.
+    // As tail_forward: warp 0 applies the block's U^-1, the other warps
+    // update the rows above it, their first row loaded before that product.
     const int nt = (int)blockDim.x - 32, t = (int)threadIdx.x - 32;
     for (int jb = ((D - 1) / 32) * 32; jb >= 0; jb -= 32) {
         const int w = min(32, D - jb);
         const long long ta = clock64();
         const bool pre = t >= 0 && t < jb;
         VT v[32];
-        const int lr_ = min(lane, w - 1);
-        if (warp == 0 || pre) tail_load_regs<VT>(T + (size_t)jb * ld + (warp == 0 ? jb + lr_ : t), ld, w, v);
+        if (warp == 0) tail_load_regs<VT>(Ti + (size_t)(jb >> 5) * 2048 + 1024 + lane, 32, 32, v);
+        else if (pre) tail_load_regs<VT>(T + (size_t)jb * ld + t, ld, w, v);
         if (warp == 0) {
-            const double dgv = ValTraits<VT>::load(T + (size_t)(jb + lr_) * ld + jb + lr_);
-            const double rdg = lane < w ? 1.0 / dgv : 1.0;
-            double yr = lane < w ? yt[jb + lane] : 0.0;
-#pragma unroll
-            for (int c = 31; c >= 0; c--) {
-                if (c < w) {
-                    if (lane == c) yr = yr * rdg;
-                    const double zc = __shfl_sync(0xffffffffu, yr, c);
-                    if (lane < c) yr = fma(-(double)v[c], zc, yr);
-                }
-            }
+            const double yr = lane < w ? tail_dot_regs<VT>(v, yt + jb, w) : 0.0;
+            __syncwarp();
             if (lane < w) yt[jb + lane] = yr;
         }
         __syncthreads();
@@ -1113,8 +1172,8 @@ __device__ __noinline__ void tail_backward(const PatternDev& P, const VT* T, dou
 // ---------------------------------------------------------------------------
 template <typename VT>
 __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval,
-                             const VT* udiag, const VT* tail, const double* rhs, double* y, Smem& sm,
-                             int& bad, SysStats* st) {
+                             const VT* udiag, const VT* tail, const VT* tinv, const double* rhs, double* y,
+                             Smem& sm, int& bad, SysStats* st) {
     const long long t0 = clock64();
     const int n = P.n, k0 = P.k0;
     const int lane = threadIdx.x & 31;
@@ -1149,8 +1208,8 @@ __device__ void cta_lu_apply(const PatternDev& P, const VT* lval, const VT* uval
     __syncthreads();
     const long long t1 = clock64();
     if (P.dtail > 0) {
-        tail_forward<VT>(P, tail, y, st);
-        tail_backward<VT>(P, tail, y, st);
+        tail_forward<VT>(P, tail, tinv, y, st);
+        tail_backward<VT>(P, tail, tinv, y, st);
     }
     const long long t2 = clock64();
     // Rows of the dense tail are complete before the sparse U sweep starts.
@@ -1568,8 +1627,8 @@ __device__ void cta_lu_apply_levels(const SysDev& S, const PatternDev& P, const 
                                        (const VT*)S.lval, nullptr, y, stage, plan.sc_ent, plan.sc_rows, part, &S.stats->status);
     const long long t1 = clock64();
     if (P.dtail > 0) {
-        tail_forward<VT>(P, (const VT*)S.tail, y, S.stats);
-        tail_backward<VT>(P, (const VT*)S.tail, y, S.stats);
+        tail_forward<VT>(P, (const VT*)S.tail, (const VT*)S.tinv, y, S.stats);
+        tail_backward<VT>(P, (const VT*)S.tail, (const VT*)S.tinv, y, S.stats);
     }
     const long long t2 = clock64();
     if (gy)
@@ -1737,8 +1796,8 @@ __device__ void cta_lu_apply_flow(const SysDev& S, const PatternDev& P, const Sw
     __syncthreads();
     const long long t1 = clock64();
     if (P.dtail > 0) {
-        tail_forward<VT>(P, (const VT*)S.tail, y, S.stats);
-        tail_backward<VT>(P, (const VT*)S.tail, y, S.stats);
+        tail_forward<VT>(P, (const VT*)S.tail, (const VT*)S.tinv, y, S.stats);
+        tail_backward<VT>(P, (const VT*)S.tail, (const VT*)S.tinv, y, S.stats);
     }
     for (int i = threadIdx.x; i < n; i += blockDim.x)
         ((long long*)y2)[i] = i < k0 ? kFlowSentinel : __double_as_longlong(y[i]);
@@ -1777,8 +1836,8 @@ __device__ __forceinline__ void lu_apply(const SysDev& S, const SmemPlan& plan, 
     if (plan.flow && sd && P.n <= plan.ycap)
         cta_lu_apply_flow<VT>(S, P, *sd, rhs, y, flow_y2_base(plan, sm), flow_ring_base(plan, sm), sm, bad);
     else if (sd) cta_lu_apply_levels<VT>(S, P, plan, rhs, y, *sd, sweep_stage_base(plan, sm), sm.red);
-    else cta_lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, (const VT*)S.tail, rhs,
-                          y, sm, bad, S.stats);
+    else cta_lu_apply<VT>(P, (const VT*)S.lval, (const VT*)S.uval, (const VT*)S.udiag, (const VT*)S.tail,
+                          (const VT*)S.tinv, rhs, y, sm, bad, S.stats);
 }
 
 // The sweep descriptors of a solve: loaded into shared memory when they fit
