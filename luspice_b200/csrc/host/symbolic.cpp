@@ -209,13 +209,16 @@ void levels_and_order(int n, const std::vector<int>& visit,
 // fitted to measurements on B200: the sparse engine costs about a cycle per
 // gathered update plus a latency per level of the column schedule (the
 // solve sweeps have a similar depth and each application pays it twice);
-// the dense block costs its multiply-subtract pairs (D^3 / 3), the solves'
-// reads of the dense factor (D^2 per application) and a latency per column
-// (the panel chain and the blocked solves).
+// the dense block costs its multiply-subtract pairs (D^3 / 3; the two CTAs
+// of the dense kernel's cluster share them), the solves' reads of the dense
+// factor (D^2 per application) and a latency per column (the panel chain
+// and the blocked solves).  Measured optima on B200 (50 systems, D in steps
+// of 32): the n = 4050 grid 320, the n = 989 and n = 4000 analog circuits
+// 96; the model picks those.
 int choose_dense_tail(const StaticPattern& S) {
     const int n = S.n;
     if (n < 32) return 0;
-    const double c_upd = 1.0, c_lev = 28000.0, c_cube = 0.03, c_sq = 20.0, c_lin = 2500.0;
+    const double c_upd = 1.0, c_lev = 28000.0, c_cube = 0.02, c_sq = 20.0, c_lin = 2500.0;
     // Updates that stay in the sparse engine for a tail starting at k0:
     // those whose dependency column j lies before k0.  Column j feeds
     // |L(:,j)| updates into each of the |U(j,:)| later columns.
