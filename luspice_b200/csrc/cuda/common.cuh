@@ -92,6 +92,34 @@ __device__ __forceinline__ double block_sum(double v, double* scratch) {
     return scratch[32];
 }
 
+// Two block-wide sums in one reduction (same order as block_sum for each).
+// Blocks of at most 16 warps; scratch: >= 34 doubles.
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    __syncthreads();
+    if (lane == 0) {
+        scratch[warp] = a;
+        scratch[16 + warp] = b;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        double s = lane < nw ? scratch[lane] : 0.0;
+        double t = lane < nw ? scratch[16 + lane] : 0.0;
+        s = warp_sum(s);
+        t = warp_sum(t);
+        if (lane == 0) {
+            scratch[32] = s;
+            scratch[33] = t;
+        }
+    }
+    __syncthreads();
+    a = scratch[32];
+    b = scratch[33];
+}
+
 // Block-wide maximum / minimum (all threads call, all receive the result).
 __device__ __forceinline__ double block_max(double v, double* scratch) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -2080,10 +2080,54 @@ __device__ void direct_phase(const SysDev& S, const SmemPlan& plan, char* smem_b
     __syncthreads();
 }
 
+// Arnoldi orthogonalization of w against the first j + 1 basis vectors
+// (V_i at V + i n) for j < kFusedDots, every thread on every dot product.
+// Both helpers are calls: inlined into the GMRES loop, their addresses stay
+// live across the preconditioner application and the level sweeps it calls
+// run out of registers (spill loads in every level step).
+constexpr int kFusedDots = 3;
+
+// d[i] = V_i . w (i <= j) and, when wsq is given, |w|^2 from one sweep over
+// the vectors; all threads receive the sums.
+__device__ __noinline__ void cgs_dots(const double* V, int n, int j, const double* w, double* d, double* wsq,
+                                      Smem& sm) {
+    double s[kFusedDots + 1];
+#pragma unroll
+    for (int i = 0; i <= kFusedDots; i++) s[i] = 0.0;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const double we = w[e];
+        if (wsq) s[kFusedDots] = fma(we, we, s[kFusedDots]);
+#pragma unroll
+        for (int i = 0; i < kFusedDots; i++)
+            if (i <= j) s[i] = fma(V[(size_t)i * n + e], we, s[i]);
+    }
+    block_sum2(s[0], s[kFusedDots], sm.red);
+    if (j >= 1) block_sum2(s[1], s[2], sm.red);
+#pragma unroll
+    for (int i = 0; i < kFusedDots; i++) d[i] = i <= j ? s[i] : 0.0;
+    if (wsq) *wsq = s[kFusedDots];
+}
+
+// w -= sum_{i <= j} d[i] V_i; returns the new |w|^2 (all threads).
+__device__ __noinline__ double cgs_update(const double* V, int n, int j, const double* d, double* w, Smem& sm) {
+    double nrm = 0.0;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        double acc = w[e];
+#pragma unroll
+        for (int i = 0; i < kFusedDots; i++)
+            if (i <= j) acc = fma(-d[i], V[(size_t)i * n + e], acc);
+        w[e] = acc;
+        nrm = fma(acc, acc, nrm);
+    }
+    return block_sum(nrm, sm.red);
+}
+
 // ---------------------------------------------------------------------------
 // GMRES-IR: restarted, right-preconditioned GMRES on P A Q with the stored
 // factors as preconditioner (VT), inner products A z with AT values; outer
-// residual b - A x, Arnoldi (classical Gram-Schmidt, two passes), Givens
+// residual b - A x, Arnoldi (classical Gram-Schmidt: for the first
+// kFusedDots basis vectors a second pass only when the first cancels more
+// than half of |w|^2, beyond them always two passes), Givens
 // rotations, least-squares update and solution update in fp64.
 // Workspace (doubles): bt, xt, r, z, w, yg (n each), V ((m+1) n), xprev (n).
 // ---------------------------------------------------------------------------
@@ -2208,28 +2252,55 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
             }
             __syncthreads();
             if (threadIdx.x == 0) S.stats->cyc_spmv += clock64() - tsp;
-            const double wn0 = sqrt(cta_dot(w, w, n, sm));
-            for (int pass = 0; pass < 2; pass++) {
-                for (int i = warp; i <= j; i += nw) {
-                    const double* vi = V + (size_t)i * n;
-                    double s = 0.0;
-                    for (int e = lane; e < n; e += 32) s = fma(vi[e], w[e], s);
-                    s = warp_sum(s);
-                    if (lane == 0) {
-                        yc[i] = s;
-                        if (pass == 0) h[i] = s;
-                        else H[(size_t)i * m + j] = h[i] + s;
+            double wn0, hn;
+            if (j < kFusedDots) {
+                // Classical Gram-Schmidt against V_0..V_j, all threads on
+                // every dot product: one sweep for the dots and |w|^2, one
+                // for the update and the new |w|^2; the second pass only
+                // when the first cancelled more than half of |w|^2 (Daniel,
+                // Gragg, Kaufman and Stewart's reorthogonalization test).
+                double d[kFusedDots];
+                double wsq;
+                cgs_dots(V, n, j, w, d, &wsq, sm);
+                wn0 = sqrt(wsq);
+                double hsq = cgs_update(V, n, j, d, w, sm);
+                if (hsq < 0.5 * wsq) {
+                    double d2[kFusedDots];
+                    cgs_dots(V, n, j, w, d2, nullptr, sm);
+                    hsq = cgs_update(V, n, j, d2, w, sm);
+#pragma unroll
+                    for (int i = 0; i < kFusedDots; i++) d[i] += d2[i];
+                }
+                if (threadIdx.x == 0) {
+#pragma unroll
+                    for (int i = 0; i < kFusedDots; i++)
+                        if (i <= j) H[(size_t)i * m + j] = d[i];
+                }
+                hn = sqrt(hsq);
+            } else {
+                wn0 = sqrt(cta_dot(w, w, n, sm));
+                for (int pass = 0; pass < 2; pass++) {
+                    for (int i = warp; i <= j; i += nw) {
+                        const double* vi = V + (size_t)i * n;
+                        double s = 0.0;
+                        for (int e = lane; e < n; e += 32) s = fma(vi[e], w[e], s);
+                        s = warp_sum(s);
+                        if (lane == 0) {
+                            yc[i] = s;
+                            if (pass == 0) h[i] = s;
+                            else H[(size_t)i * m + j] = h[i] + s;
+                        }
                     }
+                    __syncthreads();
+                    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+                        double acc = w[e];
+                        for (int i = 0; i <= j; i++) acc = fma(-yc[i], V[(size_t)i * n + e], acc);
+                        w[e] = acc;
+                    }
+                    __syncthreads();
                 }
-                __syncthreads();
-                for (int e = threadIdx.x; e < n; e += blockDim.x) {
-                    double acc = w[e];
-                    for (int i = 0; i <= j; i++) acc = fma(-yc[i], V[(size_t)i * n + e], acc);
-                    w[e] = acc;
-                }
-                __syncthreads();
+                hn = sqrt(cta_dot(w, w, n, sm));
             }
-            const double hn = sqrt(cta_dot(w, w, n, sm));
             inner_total++;
             jj = j + 1;
             const bool breakdown = !(hn > 1e-14 * wn0) || hn == 0.0;
