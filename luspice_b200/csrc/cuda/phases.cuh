@@ -2339,22 +2339,21 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
             }
         }
         __syncthreads();
+        // The correction sum_i y_i z_i, applied as it is formed.
+        double sy = 0.0, sx = 0.0;
         for (int e = threadIdx.x; e < n; e += blockDim.x) {
             double acc = 0.0;
             for (int i = 0; i < jj; i++) acc = fma(yc[i], Zb[(size_t)i * n + e], acc);
-            y[e] = acc;
-        }
-        __syncthreads();
-        double sy = 0.0, sx = 0.0;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            xprev[e] = xt[e];
-            const double xn = xt[e] + y[e];
+            const double xo = xt[e];
+            xprev[e] = xo;
+            const double xn = xo + acc;
             xt[e] = xn;
-            sy = fma(y[e], y[e], sy);
+            sy = fma(acc, acc, sy);
             sx = fma(xn, xn, sx);
         }
-        const double ny = sqrt(block_sum(sy, sm.red));
-        const double nx = sqrt(block_sum(sx, sm.red));
+        block_sum2(sy, sx, sm.red);
+        const double ny = sqrt(sy);
+        const double nx = sqrt(sx);
         const double dx = nx > 0.0 ? ny / nx : ny;
         if (dx_prev > 0.0) {
             const double rho = fmin(dx / dx_prev, 0.99);
