@@ -88,7 +88,9 @@ typedef struct {
     int rung;                      /* what produced the result: 0 the batch's own
                                       precision, 1 ladder P-safe, 2 ladder P-hard */
     /* SM cycles summed over warps: refactor waits for dependency columns,
-     * gathers of their L parts, updates; refactor wall cycles of the CTA */
+     * gathers of their L parts, updates (0 unless the library is built with
+     * -DLUSP_REFACTOR_PHASE_CYCLES=1: the clock reads cost ~3 % of the
+     * refactor); refactor wall cycles of the CTA (always) */
     long long cyc_wait, cyc_gather, cyc_update, cyc_refactor;
     /* SM cycles of the solve phase (CTA wall time): L sweeps, dense-tail
      * solves, U sweeps, SpMVs, the whole solve */

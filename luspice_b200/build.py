@@ -43,8 +43,12 @@ def _cmd(src: str) -> tuple[list[str], Path]:
     elif src.endswith(".cpp"):
         cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", *inc, "-c", str(path), "-o", str(obj)]
     else:
+        # LUSP_REFACTOR_PHASE_CYCLES=1 in the environment: the refactor's
+        # per-phase cycle counters (diagnostics, ~3 % of its time; rebuild
+        # with --force after changing it).
+        opt = ["-DLUSP_REFACTOR_PHASE_CYCLES=1"] if os.environ.get("LUSP_REFACTOR_PHASE_CYCLES") == "1" else []
         cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC",
-               "-Xcompiler", "-ffp-contract=off", *inc, "-c", str(path), "-o", str(obj)]
+               "-Xcompiler", "-ffp-contract=off", *opt, *inc, "-c", str(path), "-o", str(obj)]
     return cmd, obj
 
 

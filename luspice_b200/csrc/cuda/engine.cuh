@@ -80,7 +80,8 @@ struct SysStats {
     int rung;                // ladder rung of the result: 0 P-fast (the batch's
                              // own precision), 1 P-safe, 2 P-hard
     // SM cycles (summed over warps): refactor waits for dependency columns,
-    // gathers of their L parts, updates; refactor wall cycles of the CTA.
+    // gathers of their L parts, updates (0 unless built with
+    // LUSP_REFACTOR_PHASE_CYCLES); refactor wall cycles of the CTA.
     long long cyc_wait, cyc_gather, cyc_update, cyc_refactor;
     // SM cycles of the solve (CTA wall time, summed over calls): L sweeps,
     // dense-tail solves, U sweeps, SpMVs, whole solve phase.
