@@ -382,8 +382,10 @@ int lusp_sell_info(const lusp_sell *s, long *stored, long *nnz, double *fp16_sca
 /* ---- autotuning (measured on this GPU) ---- */
 /* Times refactor + solve of nsys copies of (Ax, b) for candidate
  * configurations — dense trailing block (none, the cost model's choice,
- * half of it, larger), refactor CTA size (the automatic one and its
- * neighbour), refactor cluster size (1, 2), solve-kernel CTA (256, 512
+ * half of it, larger), refactor shape (the engine's own rules, returned as
+ * refactor_threads = refactor_cluster = 0, which also choose spread mode for
+ * a batch of medium systems; or an explicit CTA size, the automatic one and
+ * its neighbour, on cluster sizes 1 and 2), solve-kernel CTA (256, 512
  * threads) and sweep kind (level-synchronous, dataflow) — and
  * returns the fastest: *opts is updated (its other fields are kept),
  * *dense_tail is the block size to pass to lusp_pattern_create_ex, and

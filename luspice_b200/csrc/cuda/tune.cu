@@ -81,17 +81,22 @@ int lusp_tune(int n, const int* Ap, const int* Ai, const double* Ax, const doubl
         lusp_pattern* P = nullptr;
         if (lusp_pattern_create_ex(n, Ap, Ai, Ax, nullptr, d, &P) != LUSP_OK) continue;
         std::vector<lusp_pattern*> pats(nsys, P);
-        // Refactor CTA: the automatic size and its neighbour (one CTA per SM
-        // when every system has an SM, else two per SM).
+        // Refactor shape: the engine's own rules (0, 0: which also choose
+        // spread mode for a batch of medium systems, at most one per SM),
+        // then explicit CTA sizes (the automatic one and its neighbour: one
+        // CTA per SM when every system has an SM, else two per SM) on lone
+        // CTAs and 2-CTA clusters.
         const bool few = nsys <= lusp::sm_count();
         const int rts[2] = {few ? 768 : 512, few ? 1024 : 768};
+        std::vector<std::pair<int, int>> shapes{{0, 0}};
         for (int rt : rts)
-        for (int rcl : {1, 2})
+            for (int rcl : {1, 2}) shapes.push_back({rt, rcl});
+        for (const auto& shp : shapes)
             for (int bt : {256, 512})
                 for (int sw : {0, 1}) {
                     lusp_batch_opts o = *opts;
-                    o.refactor_threads = rt;
-                    o.refactor_cluster = rcl;
+                    o.refactor_threads = shp.first;
+                    o.refactor_cluster = shp.second;
                     o.block_threads = bt;
                     o.ctas_per_sm = bt == 512 ? 1 : 2;
                     o.solve_sweep = sw;

@@ -34,8 +34,10 @@ def test_tune_power_grid(gpu):
     nsys = 8
     t = api.autotune(m, nsys)
     assert 0 <= t["dense_tail"] <= 768 and t["ms"] > 0
-    assert t["opts"]["refactor_cluster"] in (1, 2) and t["opts"]["block_threads"] in (256, 512)
-    assert t["opts"]["refactor_threads"] in (512, 768, 1024)
+    # 0, 0: the engine's own refactor rules (spread mode for this batch).
+    assert t["opts"]["refactor_cluster"] in (0, 1, 2) and t["opts"]["block_threads"] in (256, 512)
+    assert t["opts"]["refactor_threads"] in (0, 512, 768, 1024)
+    assert (t["opts"]["refactor_threads"] == 0) == (t["opts"]["refactor_cluster"] == 0)
     assert t["opts"]["solve_sweep"] in (0, 1)
     vals = m.perturbed(nsys, seed=77)
     P = api.Pattern.from_matrix(m, dense_tail=t["dense_tail"])
