@@ -179,7 +179,7 @@ __device__ void dense_tail_factor(const PatternDev& P, double* W, Smem& sm, cons
                                   const SolveParams& prm, double& minpiv, double& minratio, int& bad,
                                   SysStats* st) {
     namespace cgr = cooperative_groups;
-    const int crank = CL ? (int)cgr::this_cluster().block_rank() : 0, csize = CL ? 2 : 1;
+    const int crank = CL ? (int)cgr::this_cluster().block_rank() : 0;
     const bool lead = crank == 0;
     const int D = P.dtail, ld = P.tail_ld, k0 = P.k0, nb = plan.tnb;
     const int ps = nb + 1;   // panel row stride: odd, so a lane per row hits distinct banks
@@ -622,7 +622,7 @@ __device__ __forceinline__ void cp_async_16(void* sdst, const void* gsrc) {
 __device__ void spread_finish(const SysDev& S, unsigned* sync, int group, Smem& sm, double minpiv,
                               double minratio, double maxu, int bad, long long cw, long long cg, long long cu,
                               long long t_begin) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
     int* ctl = (int*)sync;
     unsigned long long* acc = (unsigned long long*)(sync + kSyncAcc);
     minpiv = warp_min(minpiv);
@@ -640,7 +640,6 @@ __device__ void spread_finish(const SysDev& S, unsigned* sync, int group, Smem& 
     }
     __threadfence();
     __syncthreads();
-    (void)nw;
     (void)sm;
     if (threadIdx.x == 0 && atomicAdd(&ctl[kSyncDone], 1) == group - 1) {
         __threadfence();
@@ -2178,8 +2177,6 @@ __device__ void gmres_phase(const SysDev& S, const SmemPlan& plan, char* smem_ba
     double* h = sn + m;
     double* yc = h + (m + 1);
     double* y = (n <= plan.ycap) ? ys : yg;
-    const VT* lval = (const VT*)S.lval;
-    const VT* uval = (const VT*)S.uval;
     const VT* udiag = (const VT*)S.udiag;
     const VT* tail = (const VT*)S.tail;
     constexpr bool kHalf = std::is_same<AT, __half>::value;
